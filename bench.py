@@ -1,0 +1,395 @@
+"""Benchmark of the simulation hot path on one node.
+
+Workload (phase-contrast flow, the metric's configuration): a 200k-node P1
+tube (radius 12 mm, length 100 mm) with Poiseuille flow (peak 1 m/s) moving
+the nodes as a rank-1 PODVelocity, off-resonance ~N(0, 20 Hz), T1 ~ U[0.8,
+1.2] s, T2 ~ U[50, 100] ms, lumped P1 mass weights, a 3-D Cartesian
+96 x 96 x 32 readout (FOV 0.1 m, sample time set by the readout index, so 96
+distinct times) and 4 velocity encodings (reference + 3 axes, VENC 1.5 m/s).
+
+One step simulates one cardiac frame: the fused Bloch sweep of the
+phase-contrast imaging block for the 4 encodings (final-state form, motion on
+the GPU), then the mass-weighted NUDFT of the 4 encodings at once
+(V = 4 columns).  Units: node*k-sample = nodes x k-space samples per step.
+Each rank simulates its own frame (frames are independent): weak scaling, no
+collective on the data path.  Inputs are synthetic and seeded.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3|f32]
+  python bench.py --impl reference ...   (CPU restatement of the reference)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "node*k-sample/s"
+N_NODES = 200_000
+RES = (96, 96, 32)
+FOV = (0.1, 0.1, 0.1)
+RADIUS, LENGTH = 0.012, 0.1
+VENC = 1.5
+
+
+def build_case(seed: int = 0):
+    """Host-side synthetic inputs (numpy)."""
+    from feelmri_b200 import workloads as W
+    mesh = W.tube(N_NODES, RADIUS, LENGTH)
+    N = mesh.n_nodes
+    T1, T2 = W.tissue(N, seed)
+    phi = W.off_resonance(N, 20.0, seed + 1)
+    traj = W.cartesian(res=RES, fov=FOV)
+    vel = W.poiseuille_velocity(mesh.nodes, RADIUS, v_max=1.0, period=1000.0, n_frames=20)
+    blocks = [W.pc_imaging_block(0.0, enc, venc=VENC) for enc in W.PC_ENCODINGS]
+    return dict(mesh=mesh, N=N, T1=T1, T2=T2, phi=phi, traj=traj, vel=vel, blocks=blocks,
+                dB=np.zeros(N, np.float32))
+
+
+# --------------------------------------------------------------- clocks --
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------- GPU arm --
+
+def run_gpu(args) -> dict | None:
+    import torch
+    import scipy.sparse as sp
+    from feelmri_b200 import _lib, ops
+    from feelmri_b200._motion import lower
+    from feelmri_b200.Assemble import mass_lumped
+    from feelmri_b200.Bloch import BlochSolver
+    from feelmri_b200.FiniteElements import FiniteElement, QuadratureRule
+    from feelmri_b200.MRI import Signal
+    from feelmri_b200 import workloads as W
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    case = build_case()
+    N = case["N"]
+    traj = case["traj"]
+    S = traj.n_samples
+    V = len(W.PC_ENCODINGS)
+    vel = case["vel"]
+    frame_ms = 40.0
+    vel.update_timeshift(frame_ms * rank)
+
+    # one-time setup (untimed, as the reference assembles the mass "just once")
+    fe, qr = FiniteElement(), QuadratureRule(order=2)
+    w = mass_lumped(case["mesh"].elems, case["mesh"].nodes, fe, qr)
+    up = lambda a, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dt)  # noqa
+    r0 = up(case["mesh"].nodes.astype(np.float32))
+    T1, T2, dB = up(case["T1"]), up(case["T2"]), up(case["dB"])
+    blocks = []
+    for b in case["blocks"]:
+        blocks.append((up(b.rf, torch.complex64), up(b.G), up(b.dt.astype(np.float32)), b.t0))
+    Minds = ops.SparseCSC((N, N), up(np.arange(N + 1, dtype=np.int32), torch.int32),
+                          up(np.arange(N, dtype=np.int32), torch.int32), up(w.astype(np.float32)))
+    sig_in = ops.SignalInputs(M=Minds, kx=up(traj.kx), ky=up(traj.ky), kz=up(traj.kz), t=up(traj.t), r0=r0,
+                              phi=up(case["phi"]), T2=T2, Mxy=torch.empty((N, V), dtype=torch.complex64, device=dev))
+    Mz_tmp = torch.empty((N,), dtype=torch.float32, device=dev)
+    zero_m = torch.zeros((N,), dtype=torch.complex64, device=dev)
+    one_z = torch.ones((N,), dtype=torch.float32, device=dev)
+    out = torch.empty((*traj.shape, V), dtype=torch.complex64, device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    precision = args.precision
+
+    def step():
+        for e, (rf, G, dt, t0) in enumerate(blocks):
+            vel.update_timeshift(frame_ms * rank + t0)
+            motion = lower(vel, N, dev)
+            inp = ops.BlochInputs(r0=r0, T1=T1, T2=T2, delta_B=dB, M0=1.0, gamma=W.GAMMA, rf=rf, G=G, dt=dt,
+                                  Mxy0=zero_m, Mz0=one_z)
+            # each encoding's final transverse magnetisation lands in column e
+            ops.bloch_solve(inp, motion, history=False, Mxy_final=sig_in.Mxy[:, e], Mz_final=Mz_tmp)
+        vel.update_timeshift(frame_ms * rank)
+        return ops.signal(sig_in, lower(vel, N, dev), precision, out=out)
+
+    stream = torch.cuda.current_stream(dev)
+    ctx = ops.ctx_for(dev)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    _lib.timing_reset(ctx)
+    _lib.timing(ctx, True)
+    launches0 = _lib.launch_count()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize(dev)
+        for i in range(args.steps):
+            flush.zero_()  # L2 (126 MB) flushed between timed steps, outside the events
+            starts[i].record(stream)
+            step()
+            ends[i].record(stream)
+        torch.cuda.synchronize(dev)
+    launches = _lib.launch_count() - launches0
+    _lib.timing(ctx, False)
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    kname = "signal_tc" if precision == "bf16x3" else "signal_f32"
+    k_ms, k_n = _lib.timing_query(ctx, kname)
+    b_ms, b_n = _lib.timing_query(ctx, "bloch")
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    # correctness spot check of this run's output against FP64 (a few samples)
+    from oracle import fp64
+    Mxy_host = sig_in.Mxy.cpu().numpy()
+    idx = np.random.default_rng(0).choice(S, 256, replace=False)
+    disp = None
+    M_host = sp.diags(w).tocsc()
+    calls = np.unique(traj.t.reshape(-1)[idx])
+    from feelmri_b200.MRI import signal_call_times
+    run_times = signal_call_times(traj.t)[1:]
+    disp = np.stack([vel(float(t)) for t in run_times])
+    ref = fp64.signal(M_host, traj.kx, traj.ky, traj.kz, traj.t, case["mesh"].nodes.astype(np.float32),
+                      case["phi"], case["T2"], Mxy_host, disp=disp, pi_mode="float", sample_idx=idx)
+    got = out.cpu().numpy().reshape(S, V)[idx]
+    rel = fp64.rel_l2(got, ref)
+
+    result = None
+    if rank == 0:
+        units = float(N) * S * world
+        value = units / (total_ms / args.steps / 1e3)
+        # roofline of the dominant kernel
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() \
+            else {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "note": "fallback"}
+        k_avg_s = (k_ms / max(k_n, 1)) / 1e3
+        if precision == "bf16x3":
+            flops = 3 * 8.0 * V * float(N) * S  # issued split-BF16 MMA flops per launch
+            roof = {"bound": "tensor", "achieved": flops / k_avg_s / 1e12, "peak": peaks["bf16_tflops"],
+                    "unit": "TFLOP/s"}
+        else:
+            flops = (8.0 + 8.0 * V) * float(N) * S  # algorithmic FP32 flops per launch (phase + complex MACs)
+            roof = {"bound": "tensor", "achieved": flops / k_avg_s / 1e12, "peak": peaks["bf16_tflops"],
+                    "unit": "TFLOP/s"}
+        roof["frac"] = roof["achieved"] / roof["peak"]
+        roof["traffic"] = None
+        roof["kernel"] = kname
+        roof["kernel_ms"] = k_ms / max(k_n, 1)
+        roof["peak_source"] = "measured" if "note" not in peaks else "fallback"
+        result = {
+            "metric": METRIC, "value": value, "unit": "node*k-sample/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3" if precision == "bf16x3" else "f32",
+            "data": "synthetic (seeded mesh, tissue, flow and trajectory)",
+            "config": {"workload": "phase-contrast flow: 200k-node P1 tube, Poiseuille 1 m/s, 96x96x32 Cartesian, "
+                                   "4 velocity encodings (VENC 1.5 m/s), off-resonance N(0,20 Hz)",
+                       "nodes": N, "k_samples": S, "columns": V, "distinct_times": 96,
+                       "precision": precision, "l2": "flushed (512 MB write) between timed steps",
+                       "parallelism": f"frames x{world}" if world > 1 else "single GPU"},
+            "rel_l2_vs_fp64": rel,
+            "roofline": roof,
+            "bloch_ms_per_step": b_ms / args.steps,
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+        }
+        if args.e2e:
+            result["e2e"] = run_e2e(args, case, w, precision)
+        if args.cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(case, w, budget_s=args.cpu_seconds)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def run_e2e(args, case, w, precision) -> dict:
+    """Same step through the public API with host (numpy) buffers: the
+    sequence driver for the 4 encodings, then MRI.Signal."""
+    import scipy.sparse as sp
+    import torch
+    from feelmri_b200.Bloch import BlochSolver
+    from feelmri_b200.MRI import Signal
+    from feelmri_b200 import workloads as W
+    N = case["N"]
+    traj = case["traj"]
+    M = sp.lil_matrix((N, N), dtype=np.float64)
+    M.setdiag(w)
+    nodes32 = case["mesh"].nodes.astype(np.float32)
+
+    def step():
+        cols = []
+        for b in case["blocks"]:
+            s = BlochSolver([b], nodes32, M0=1.0, T1=case["T1"], T2=case["T2"], delta_B=case["dB"],
+                            gamma=W.GAMMA, pod_trajectory=case["vel"])
+            m, _ = s.solve()
+            cols.append(m[:, 0])
+        Mxy = np.stack(cols, axis=1)
+        case["vel"].update_timeshift(0.0)
+        K = Signal(0, M, traj.points, traj.t, nodes32, case["phi"], case["T2"], Mxy, case["vel"],
+                   precision=precision if precision == "bf16x3" else None)
+        return K
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        step()
+    torch.cuda.synchronize()
+    n = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(n):
+        K = step()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / n
+    h2d = (nodes32.nbytes * 2 + case["T1"].nbytes + case["T2"].nbytes * 2 + case["dB"].nbytes + case["phi"].nbytes
+           + sum(b.rf.nbytes + b.G.nbytes + b.dt.astype(np.float32).nbytes for b in case["blocks"])
+           + sum(p.nbytes for p in traj.points) + traj.t.nbytes + N * 4 * 8 + N * 8 + (N + 1) * 4 + N * 4)
+    d2h = K.nbytes + 4 * N * (8 + 4)
+    return {"value": float(N) * traj.n_samples / dt, "unit": "node*k-sample/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "timer": "host wall clock around the public calls, device synchronised"}
+
+
+# -------------------------------------------------------- CPU baseline --
+
+def cpu_baseline(case, w, budget_s: float = 15.0, threads: int | None = None) -> dict:
+    """The C restatement of the reference's Signal (reference compiler flags,
+    one thread per core over node ranges, partial k-spaces summed as
+    gather_data does) on a bounded sample: all nodes x a subset of readout
+    indices, sized to a few seconds of CPU work, scaled to node*k-samples/s."""
+    import oracle
+    import scipy.sparse as sp
+    traj = case["traj"]
+    N = case["N"]
+    threads = threads or max(1, os.cpu_count() or 1)
+    M = sp.diags(w.astype(np.float32)).tocsc()
+    Mxy = (np.ones((N, 4)) * (0.1 + 0.05j)).astype(np.complex64)
+    nodes32 = case["mesh"].nodes.astype(np.float32)
+    n_ro = 1
+    while True:
+        sl = slice(0, n_ro)
+        kx, ky, kz, t = (a[sl] for a in (*traj.points, traj.t))
+        disp = np.stack([case["vel"](float(tt)) for tt in np.unique(t)])
+        t0 = time.perf_counter()
+        oracle.signal(M, kx, ky, kz, t, nodes32, case["phi"], case["T2"], Mxy, disp=disp, dtype=np.float32,
+                      threads=threads, flavour="fast")
+        el = time.perf_counter() - t0
+        if el > budget_s / 4 or n_ro >= traj.shape[0]:
+            break
+        n_ro = min(traj.shape[0], max(n_ro * 2, int(n_ro * budget_s / 4 / max(el, 1e-3))))
+    samples = int(np.prod(kx.shape))
+    return {"value": float(N) * samples / el, "unit": "node*k-sample/s", "cores": threads, "kind": "port",
+            "sample": f"all {N} nodes x {samples} k-samples ({n_ro} readout indices of 96), 4 columns, "
+                      f"Signal only, {el:.1f} s"}
+
+
+def run_reference(args) -> dict | None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    case = build_case()
+    from feelmri_b200 import workloads as W
+    from oracle import fp64
+    w = fp64.lumped_p1(case["mesh"].elems, case["mesh"].nodes)
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(case, w, budget_s=4.0)
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(case, w, budget_s=max(4.0, args.cpu_seconds / max(args.steps, 1))))
+    v = statistics.median(x["value"] for x in vals)
+    cb = dict(vals[-1])
+    cb["value"] = v
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "node*k-sample/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(case["N"]) * case["traj"].n_samples / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded mesh, tissue, flow and trajectory)",
+            "config": {"workload": "phase-contrast flow: 200k-node P1 tube, Poiseuille 1 m/s, 96x96x32 Cartesian, "
+                                   "4 velocity encodings (VENC 1.5 m/s), off-resonance N(0,20 Hz)",
+                       "implementation": "CPU restatement of the reference's Signal (the reference's native "
+                                         "modules cannot be built here: Eigen is fetched from the network)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "node*k-sample/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "bf16x3"])
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    res = run_reference(args) if args.impl == "reference" else run_gpu(args)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,314 @@
+// Bloch rotation + relaxation sweep with fused POD motion.
+//
+// Restates solve_mri<float> (cpp/feelmri/BlochSimulator.cpp:12-148 with a
+// motion callable, :151-277 without) as one pass: one thread per node keeps
+// its magnetisation, relaxation factors and motion modes in registers for
+// all time steps; per-step scalars (rf, G, dt, motion weights) are read as
+// warp-uniform loads.  Step i -> i+1 uses rf[i+1], G[i+1], dt[i+1]; dt[0] is
+// ignored; e1/e2 are recomputed only when dt changes (BlochSimulator.cpp:69-99).
+#include "motion.cuh"
+
+namespace fm {
+
+// Sequential pass over the steps: float32 running time (BlochSimulator.cpp:82-83),
+// the dt-changed flags (:72) and the motion call times.
+__global__ void bloch_prep_kernel(int64_t n_time, float gamma, const float2 *__restrict__ rf,
+                                  const float *__restrict__ G, const float *__restrict__ dt, float4 *__restrict__ sa,
+                                  float4 *__restrict__ sb, int *__restrict__ changed, double *__restrict__ call_t) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  float ti = 0.0f, dti = -1.0f;
+  const float mhg = __fmul_rn(-0.5f, gamma);
+  if (call_t) call_t[0] = 0.0;
+  for (int64_t i = 0; i + 1 < n_time; ++i) {
+    const float d = dt[i + 1];
+    changed[i] = (dti != d) ? 1 : 0;
+    dti = d;
+    ti = __fadd_rn(ti, dti);
+    if (call_t) call_t[i + 1] = (double)ti;
+    const float2 r = rf[i + 1];
+    sa[i] = make_float4(r.x, r.y, __fmaf_rn(r.x, r.x, __fmul_rn(r.y, r.y)), __fmul_rn(mhg, dti));
+    sb[i] = make_float4(G[3 * (i + 1) + 0], G[3 * (i + 1) + 1], G[3 * (i + 1) + 2], dti);
+  }
+}
+
+struct BlochDev {
+  int64_t n, n_time;
+  const float *r0, *T1, *T2, *dB;
+  float M0;
+  const float2 *Mxy0;
+  const float *Mz0;
+  const float4 *sa, *sb;
+  const int *changed;
+  MotionDev md;
+  const float *weights;  // (n_time, slots) motion weights per call
+  const float *table;    // TABLE motion: (n_time, N, 3)
+  int pod_term;          // index of the register-resident POD term, -1 if none
+  float2 *Mxy_hist;
+  float *Mz_hist;
+  float2 *Mxy_final;
+  float *Mz_final;
+  float2 *Mxy_carry;
+  int64_t final_stride;
+};
+
+// MODE: 0 static, 1 TERMS with the POD modes of one term in registers,
+//       2 TERMS read from global memory (several POD terms), 3 TABLE.
+template <int MODE, int RMAX, bool HIST>
+__global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= p.n) return;
+  const float x = p.r0[3 * n + 0], y = p.r0[3 * n + 1], z = p.r0[3 * n + 2];
+  const float db = p.dB[n];
+  const float invT1 = __frcp_rn(p.T1[n]);
+  const float invT2 = __frcp_rn(p.T2[n]);
+  float2 mxy = p.Mxy0[n];
+  float mz = p.Mz0[n];
+  const float M0 = p.M0;
+  if (HIST) {
+    p.Mxy_hist[n] = mxy;
+    p.Mz_hist[n] = mz;
+  }
+
+  float phx[RMAX > 0 ? RMAX : 1], phy[RMAX > 0 ? RMAX : 1], phz[RMAX > 0 ? RMAX : 1];
+  int r_pod = 0;
+  if (MODE == 1) {
+    const fm_motion_term &T = p.md.terms[p.pod_term];
+    r_pod = T.n_modes;
+    const float *Phi = T.modes + (size_t)n * 3 * r_pod;
+#pragma unroll
+    for (int m = 0; m < RMAX; ++m) {
+      phx[m] = (m < r_pod) ? __ldg(Phi + m) : 0.f;
+      phy[m] = (m < r_pod) ? __ldg(Phi + r_pod + m) : 0.f;
+      phz[m] = (m < r_pod) ? __ldg(Phi + 2 * r_pod + m) : 0.f;
+    }
+  }
+
+  float e1 = 0.f, e2 = 0.f;
+  const int64_t steps = p.n_time - 1;
+  for (int64_t i = 0; i < steps; ++i) {
+    const float4 a = p.sa[i];
+    const float4 b = p.sb[i];
+    if (p.changed[i]) {
+      e1 = expf(__fmul_rn(-b.w, invT1));
+      e2 = expf(__fmul_rn(-b.w, invT2));
+    }
+    float px = x, py = y, pz = z;
+    if (MODE == 1 || MODE == 2) {
+      const float *w = p.weights + (i + 1) * p.md.slots;
+      float sx = 0.f, sy = 0.f, sz = 0.f;
+      for (int k = 0; k < p.md.n_terms; ++k) {
+        const fm_motion_term &T = p.md.terms[k];
+        const float *wk = w + p.md.slot0[k];
+        float tx, ty, tz;
+        if (T.kind == FM_TERM_RESPIRATORY) {
+          const float amp = wk[0];
+          tx = __fmul_rn(amp, T.direction[0]);
+          ty = __fmul_rn(amp, T.direction[1]);
+          tz = __fmul_rn(amp, T.direction[2]);
+        } else if (MODE == 1) {
+          tx = 0.f; ty = 0.f; tz = 0.f;
+#pragma unroll
+          for (int m = 0; m < RMAX; ++m) {
+            const float wm = (m < r_pod) ? wk[m] : 0.f;
+            tx = fmaf(phx[m], wm, tx);
+            ty = fmaf(phy[m], wm, ty);
+            tz = fmaf(phz[m], wm, tz);
+          }
+        } else {
+          const int r = T.n_modes;
+          const float *Phi = T.modes + (size_t)n * 3 * r;
+          tx = 0.f; ty = 0.f; tz = 0.f;
+          for (int m = 0; m < r; ++m) {
+            const float wm = wk[m];
+            tx = fmaf(__ldg(Phi + m), wm, tx);
+            ty = fmaf(__ldg(Phi + r + m), wm, ty);
+            tz = fmaf(__ldg(Phi + 2 * r + m), wm, tz);
+          }
+        }
+        if (k == 0) { sx = tx; sy = ty; sz = tz; }
+        else { sx = __fadd_rn(sx, tx); sy = __fadd_rn(sy, ty); sz = __fadd_rn(sz, tz); }
+      }
+      px = __fadd_rn(x, sx); py = __fadd_rn(y, sy); pz = __fadd_rn(z, sz);
+    } else if (MODE == 3) {
+      const float *d = p.table + ((i + 1) * p.n + n) * 3;
+      px = __fadd_rn(x, d[0]); py = __fadd_rn(y, d[1]); pz = __fadd_rn(z, d[2]);
+    }
+    // Bz = r . G + dB  (BlochSimulator.cpp:104-107)
+    const float Bz = __fadd_rn(fmaf(pz, b.z, fmaf(py, b.y, __fmul_rn(px, b.x))), db);
+    float Bn = sqrtf(fmaf(Bz, Bz, a.z));
+    Bn = (Bn < 1e-12f) ? 1e-12f : Bn;
+    const float invB = __frcp_rn(Bn);
+    const float nz = __fmul_rn(Bz, invB);
+    const float hp = __fmul_rn(Bn, a.w);
+    float s, c;
+    sincosf(hp, &s, &c);
+    // alpha = c - i nz s ; beta = -i (rf/B) s   (BlochSimulator.cpp:114-126)
+    const float al_i = -nz * s;
+    const float nxr = __fmul_rn(a.x, invB), nxi = __fmul_rn(a.y, invB);
+    const float be_r = nxi * s, be_i = -nxr * s;
+    const float a2 = fmaf(c, c, al_i * al_i);
+    const float b2 = fmaf(be_r, be_r, be_i * be_i);
+    // conj(alpha) = c + i nz s  -> ca = (c, -al_i)
+    const float ca_r = c, ca_i = -al_i;
+    // 2 conj(a) beta Mz
+    const float t1r = 2.f * (ca_r * be_r - ca_i * be_i) * mz;
+    const float t1i = 2.f * (ca_r * be_i + ca_i * be_r) * mz;
+    // conj(a)^2 Mxy
+    const float ca2r = ca_r * ca_r - ca_i * ca_i, ca2i = 2.f * ca_r * ca_i;
+    const float t2r = ca2r * mxy.x - ca2i * mxy.y;
+    const float t2i = ca2r * mxy.y + ca2i * mxy.x;
+    // beta^2 conj(Mxy)
+    const float bb_r = be_r * be_r - be_i * be_i, bb_i = 2.f * be_r * be_i;
+    const float t3r = bb_r * mxy.x + bb_i * mxy.y;
+    const float t3i = bb_i * mxy.x - bb_r * mxy.y;
+    const float nmr = t1r + t2r - t3r;
+    const float nmi = t1i + t2i - t3i;
+    // Re(alpha beta conj(Mxy))
+    const float ab_r = c * be_r - al_i * be_i, ab_i = c * be_i + al_i * be_r;
+    const float re_abm = ab_r * mxy.x + ab_i * mxy.y;
+    const float nmz = (a2 - b2) * mz - 2.f * re_abm;
+    // relaxation (BlochSimulator.cpp:141-142)
+    mxy.x = nmr * e2;
+    mxy.y = nmi * e2;
+    mz = fmaf(nmz, e1, (1.f - e1) * M0);
+    if (HIST) {
+      p.Mxy_hist[(i + 1) * p.n + n] = mxy;
+      p.Mz_hist[(i + 1) * p.n + n] = mz;
+    }
+  }
+  if (p.Mxy_final) p.Mxy_final[n * p.final_stride] = mxy;
+  if (p.Mz_final) p.Mz_final[n] = mz;
+  if (p.Mxy_carry) p.Mxy_carry[n] = make_float2(0.f * mxy.x, 0.f * mxy.y);
+}
+
+template <int MODE, int RMAX>
+static void launch_bloch(const BlochDev &p, bool hist, cudaStream_t st) {
+  const int threads = 128;
+  const unsigned blocks = (unsigned)ceil_div(p.n, threads);
+  if (hist) bloch_kernel<MODE, RMAX, true><<<blocks, threads, 0, st>>>(p);
+  else bloch_kernel<MODE, RMAX, false><<<blocks, threads, 0, st>>>(p);
+}
+
+static void carve_bloch(Carve &c, const fm_bloch_args *a, float4 **sa, float4 **sb, int **changed, double **call_t,
+                        float **weights) {
+  const int64_t steps = a->n_time > 1 ? a->n_time - 1 : 1;
+  *sa = c.take<float4>(steps);
+  *sb = c.take<float4>(steps);
+  *changed = c.take<int>(steps);
+  *call_t = c.take<double>(a->n_time);
+  *weights = c.take<float>((size_t)a->n_time * motion_slots(a->motion));
+}
+
+static int validate_bloch(const fm_bloch_args *a) {
+  FM_REQUIRE(a != nullptr, FM_ERR_ARG, "fm_bloch_solve_f32: null args");
+  FM_REQUIRE(a->n_pos >= 0, FM_ERR_SHAPE, "fm_bloch_solve_f32: negative n_pos");
+  FM_REQUIRE(a->n_time >= 1, FM_ERR_SHAPE,
+             "fm_bloch_solve_f32: rf_all must hold at least one sample (the initial state column)");
+  FM_REQUIRE((a->Mxy_hist == nullptr) == (a->Mz_hist == nullptr), FM_ERR_ARG,
+             "fm_bloch_solve_f32: Mxy_hist and Mz_hist must be given together");
+  if (a->n_pos > 0) {
+    FM_REQUIRE(a->r0 && a->T1 && a->T2 && a->delta_B && a->Mxy0 && a->Mz0, FM_ERR_ARG,
+               "fm_bloch_solve_f32: null node array");
+  }
+  FM_REQUIRE(a->rf && a->G && a->dt, FM_ERR_ARG, "fm_bloch_solve_f32: null sequence array");
+  FM_TRY(validate_motion(a->motion, a->n_pos, "fm_bloch_solve_f32"));
+  if (a->motion && a->motion->kind == FM_MOTION_TABLE) {
+    FM_REQUIRE(a->motion->table_calls == a->n_time, FM_ERR_SHAPE,
+               "fm_bloch_solve_f32: TABLE motion holds %lld calls, the solve makes %lld",
+               (long long)a->motion->table_calls, (long long)a->n_time);
+  }
+  return FM_OK;
+}
+
+}  // namespace fm
+
+using namespace fm;
+
+extern "C" {
+
+int fm_bloch_workspace_size(const fm_bloch_args *a, size_t *bytes) {
+  FM_REQUIRE(bytes != nullptr, FM_ERR_ARG, "fm_bloch_workspace_size: null output");
+  FM_TRY(validate_bloch(a));
+  Carve c(nullptr, 0);
+  float4 *sa, *sb;
+  int *ch;
+  double *ct;
+  float *w;
+  carve_bloch(c, a, &sa, &sb, &ch, &ct, &w);
+  *bytes = c.used;
+  return FM_OK;
+}
+
+int fm_bloch_solve_f32(fm_ctx *ctx, const fm_bloch_args *a, void *workspace, size_t workspace_bytes) {
+  FM_TRY(ctx_ok(ctx));
+  FM_TRY(validate_bloch(a));
+  DeviceGuard g(ctx->device);
+  cudaStream_t st = ctx->stream;
+  Carve cv(workspace, workspace_bytes);
+  float4 *sa, *sb;
+  int *changed;
+  double *call_t;
+  float *weights;
+  carve_bloch(cv, a, &sa, &sb, &changed, &call_t, &weights);
+  FM_TRY(carve_ok(cv, "fm_bloch_solve_f32"));
+  if (a->n_pos == 0) return FM_OK;
+
+  const MotionDev md = make_motion_dev(a->motion);
+  bloch_prep_kernel<<<1, 1, 0, st>>>(a->n_time, a->gamma, reinterpret_cast<const float2 *>(a->rf), a->G, a->dt, sa,
+                                     sb, changed, md.kind == FM_MOTION_TERMS ? call_t : nullptr);
+  count_launch();
+  FM_TRY(check_launch("bloch_prep_kernel"));
+  FM_TRY(launch_motion_weights(md, call_t, a->n_time, weights, st));
+
+  BlochDev p{};
+  p.n = a->n_pos;
+  p.n_time = a->n_time;
+  p.r0 = a->r0; p.T1 = a->T1; p.T2 = a->T2; p.dB = a->delta_B;
+  p.M0 = a->M0;
+  p.Mxy0 = reinterpret_cast<const float2 *>(a->Mxy0);
+  p.Mz0 = a->Mz0;
+  p.sa = sa; p.sb = sb; p.changed = changed;
+  p.md = md;
+  p.weights = weights;
+  p.table = (a->motion && a->motion->kind == FM_MOTION_TABLE) ? static_cast<const float *>(a->motion->table) : nullptr;
+  p.Mxy_hist = reinterpret_cast<float2 *>(a->Mxy_hist);
+  p.Mz_hist = a->Mz_hist;
+  p.Mxy_final = reinterpret_cast<float2 *>(a->Mxy_final);
+  p.Mz_final = a->Mz_final;
+  p.Mxy_carry = reinterpret_cast<float2 *>(a->Mxy_carry);
+  p.final_stride = a->final_stride > 1 ? a->final_stride : 1;
+  p.pod_term = -1;
+  const bool hist = a->Mxy_hist != nullptr;
+  ScopedTimer timer(ctx, hist ? "bloch_history" : "bloch_final");
+
+  if (md.kind == FM_MOTION_NONE) {
+    launch_bloch<0, 0>(p, hist, st);
+  } else if (md.kind == FM_MOTION_TABLE) {
+    launch_bloch<3, 0>(p, hist, st);
+  } else {
+    int n_pod = 0, r = 0;
+    for (int k = 0; k < md.n_terms; ++k)
+      if (md.terms[k].kind != FM_TERM_RESPIRATORY) {
+        ++n_pod;
+        p.pod_term = k;
+        r = md.terms[k].n_modes;
+      }
+    if (n_pod == 0 || n_pod > 1 || r > 32) {
+      launch_bloch<2, 0>(p, hist, st);
+    } else if (r <= 1) {
+      launch_bloch<1, 1>(p, hist, st);
+    } else if (r <= 4) {
+      launch_bloch<1, 4>(p, hist, st);
+    } else if (r <= 8) {
+      launch_bloch<1, 8>(p, hist, st);
+    } else if (r <= 16) {
+      launch_bloch<1, 16>(p, hist, st);
+    } else {
+      launch_bloch<1, 32>(p, hist, st);
+    }
+  }
+  count_launch();
+  return check_launch("bloch_kernel");
+}
+
+}  // extern "C"

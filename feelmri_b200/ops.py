@@ -1,0 +1,307 @@
+"""Device-level entry points: torch CUDA tensors in, torch CUDA tensors out.
+
+These wrap the C ABI (include/feelmri_b200.h) with PyTorch only as the
+allocator of device buffers and the provider of the current stream.  The
+drop-in shims (BlochSimulator, MRI, Assemble, POD) convert numpy inputs with
+the reference's pybind11 rules and call into here.  No function here computes
+on the CPU; without a CUDA device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from ._motion import LoweredMotion
+
+_ws_cache: dict[tuple[int, int], torch.Tensor] = {}
+
+
+def require_cuda() -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("feelmri_b200 runs on a CUDA device (B200, sm_100a); none is available and there "
+                           "is no CPU fallback")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def ctx_for(device: torch.device) -> int:
+    """Library context of `device` bound to torch's current stream there."""
+    stream = torch.cuda.current_stream(device)
+    return L.bind_stream(device.index, stream.cuda_stream)
+
+
+def workspace(device: torch.device, nbytes: int) -> torch.Tensor:
+    """A scratch buffer of at least nbytes, cached per (device, stream).  Work
+    on one stream is ordered, so reusing the buffer there is safe."""
+    stream = torch.cuda.current_stream(device)
+    key = (device.index, stream.cuda_stream)
+    buf = _ws_cache.get(key)
+    if buf is None or buf.numel() < nbytes:
+        buf = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8, device=device)
+        _ws_cache[key] = buf
+    return buf
+
+
+def release_workspaces() -> None:
+    _ws_cache.clear()
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _check_dev(name: str, t: torch.Tensor, dtype: torch.dtype, shape: tuple, device: torch.device):
+    if t.device != device:
+        raise ValueError(f"{name} is on {t.device}, expected {device}")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} has dtype {t.dtype}, expected {dtype}")
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+# ---------------------------------------------------------------- POD GEMV --
+
+def tensordot_modes_weights(modes: torch.Tensor, weights: torch.Tensor, out: torch.Tensor | None = None):
+    """out[p, c] = sum_m modes[p, c, m] * weights[m]  (POD.cpp:5-38)."""
+    dev = modes.device
+    P, Cc, M = modes.shape
+    if out is None:
+        out = torch.empty((P, Cc), dtype=modes.dtype, device=dev)
+    _check_dev("weights", weights, modes.dtype, (M,), dev)
+    fn = L.lib().fm_pod_tensordot_f32 if modes.dtype == torch.float32 else L.lib().fm_pod_tensordot_f64
+    L.check(fn(ctx_for(dev), modes.data_ptr(), weights.data_ptr(), P, Cc, M, out.data_ptr()))
+    return out
+
+
+def motion_eval(motion: LoweredMotion, n_nodes: int, times, device: torch.device) -> torch.Tensor:
+    """Displacements (len(times), N, 3) of a lowered motion at host times."""
+    times = np.ascontiguousarray(times, dtype=np.float64)
+    out = torch.empty((len(times), n_nodes, 3), dtype=torch.float32, device=device)
+    nbytes = C.c_size_t()
+    L.check(L.lib().fm_motion_eval_workspace_size(C.byref(motion.struct), n_nodes, len(times), C.byref(nbytes)))
+    ws = workspace(device, nbytes.value)
+    L.check(L.lib().fm_motion_eval(ctx_for(device), C.byref(motion.struct), n_nodes,
+                                   times.ctypes.data_as(C.c_void_p), len(times), out.data_ptr(),
+                                   ws.data_ptr(), ws.numel()))
+    return out
+
+
+# ------------------------------------------------------------ Bloch sweep --
+
+@dataclass
+class BlochInputs:
+    """Device-resident inputs of one solve_mri call (all float32/complex64)."""
+    r0: torch.Tensor        # (N, 3)
+    T1: torch.Tensor        # (N,)
+    T2: torch.Tensor        # (N,)
+    delta_B: torch.Tensor   # (N,)
+    M0: float
+    gamma: float
+    rf: torch.Tensor        # (n_t,) complex64
+    G: torch.Tensor         # (n_t, 3)
+    dt: torch.Tensor        # (n_t,)
+    Mxy0: torch.Tensor      # (N,) complex64
+    Mz0: torch.Tensor       # (N,)
+
+
+def bloch_solve(inp: BlochInputs, motion: LoweredMotion, history: bool = True,
+                Mxy_final: torch.Tensor | None = None, Mz_final: torch.Tensor | None = None,
+                Mxy_carry: torch.Tensor | None = None, allocate_final: bool = True):
+    """Runs the fused Bloch sweep.  history=True returns the (N, n_t)
+    column-major histories (as (n_t, N) row-major tensors); otherwise the
+    final state is written to Mxy_final / Mz_final (allocated when None and
+    allocate_final) and 0 * final Mxy to Mxy_carry when given.  The output
+    buffers may alias Mxy0 / Mz0 (each node is read before it is written)."""
+    dev = inp.r0.device
+    N = inp.r0.shape[0]
+    n_t = inp.rf.shape[0]
+    _check_dev("r0", inp.r0, torch.float32, (N, 3), dev)
+    for name in ("T1", "T2", "delta_B", "Mz0"):
+        _check_dev(name, getattr(inp, name), torch.float32, (N,), dev)
+    _check_dev("Mxy0", inp.Mxy0, torch.complex64, (N,), dev)
+    _check_dev("rf", inp.rf, torch.complex64, (n_t,), dev)
+    _check_dev("G", inp.G, torch.float32, (n_t, 3), dev)
+    _check_dev("dt", inp.dt, torch.float32, (n_t,), dev)
+    a = L.BlochArgs()
+    a.n_pos, a.n_time = N, n_t
+    a.r0, a.T1, a.T2, a.delta_B = (_ptr(inp.r0), _ptr(inp.T1), _ptr(inp.T2), _ptr(inp.delta_B))
+    a.M0, a.gamma = float(np.float32(inp.M0)), float(np.float32(inp.gamma))
+    a.rf, a.G, a.dt = _ptr(inp.rf), _ptr(inp.G), _ptr(inp.dt)
+    a.Mxy0, a.Mz0 = _ptr(inp.Mxy0), _ptr(inp.Mz0)
+    a.motion = C.pointer(motion.struct)
+    hist = None
+    if history:
+        Mxy_h = torch.empty((n_t, N), dtype=torch.complex64, device=dev)
+        Mz_h = torch.empty((n_t, N), dtype=torch.float32, device=dev)
+        a.Mxy_hist, a.Mz_hist = Mxy_h.data_ptr(), Mz_h.data_ptr()
+        hist = (Mxy_h, Mz_h)
+    if Mxy_final is None and not history and allocate_final:
+        Mxy_final = torch.empty((N,), dtype=torch.complex64, device=dev)
+    if Mz_final is None and not history and allocate_final:
+        Mz_final = torch.empty((N,), dtype=torch.float32, device=dev)
+    for name, buf, dt in (("Mz_final", Mz_final, torch.float32), ("Mxy_carry", Mxy_carry, torch.complex64)):
+        if buf is not None:
+            _check_dev(name, buf, dt, (N,), dev)
+    if Mxy_final is not None:
+        # a 1-D view with any positive stride, e.g. one column of an (N, V) matrix
+        if Mxy_final.device != dev or Mxy_final.dtype != torch.complex64 or tuple(Mxy_final.shape) != (N,):
+            raise ValueError("Mxy_final must be a complex64 (N,) tensor on the solve's device")
+        if Mxy_final.stride(0) < 1:
+            raise ValueError("Mxy_final must have a positive stride")
+        a.final_stride = Mxy_final.stride(0)
+    a.Mxy_final, a.Mz_final, a.Mxy_carry = _ptr(Mxy_final), _ptr(Mz_final), _ptr(Mxy_carry)
+    nbytes = C.c_size_t()
+    L.check(L.lib().fm_bloch_workspace_size(C.byref(a), C.byref(nbytes)))
+    ws = workspace(dev, nbytes.value)
+    L.check(L.lib().fm_bloch_solve_f32(ctx_for(dev), C.byref(a), ws.data_ptr(), ws.numel()))
+    if history:
+        return hist
+    return Mxy_final, Mz_final
+
+
+# ----------------------------------------------------------------- Signal --
+
+@dataclass
+class SparseCSC:
+    """A CSC matrix on the device (int32 index arrays)."""
+    shape: tuple
+    indptr: torch.Tensor
+    indices: torch.Tensor
+    data: torch.Tensor
+
+    @property
+    def nnz(self) -> int:
+        return int(self.indices.numel())
+
+
+@dataclass
+class SignalInputs:
+    """Device-resident inputs of one Signal call.  Real arrays are float32 for
+    the F32 and BF16X3 forms and float64 for the F64 form."""
+    M: SparseCSC
+    kx: torch.Tensor      # (n_ro, n_lines, n_kz)
+    ky: torch.Tensor
+    kz: torch.Tensor
+    t: torch.Tensor       # (n_ro, n_lines, n_kz)
+    r0: torch.Tensor      # (N, 3)
+    phi: torch.Tensor     # (N,)
+    T2: torch.Tensor      # (N,)
+    Mxy: torch.Tensor     # (N, V) complex
+
+
+PRECISIONS = {"f32": L.FM_PREC_F32, "f64": L.FM_PREC_F64, "bf16x3": L.FM_PREC_BF16X3}
+
+
+def signal_args(inp: SignalInputs, motion: LoweredMotion, precision: str, out: torch.Tensor) -> L.SignalArgs:
+    real = torch.float64 if precision == "f64" else torch.float32
+    cplx = torch.complex128 if precision == "f64" else torch.complex64
+    dev = inp.r0.device
+    N = inp.r0.shape[0]
+    V = inp.Mxy.shape[1]
+    grid = tuple(inp.kx.shape)
+    if len(grid) != 3:
+        raise ValueError("k-space arrays must be 3-D (n_ro, n_lines, n_kz)")
+    for name in ("kx", "ky", "kz", "t"):
+        _check_dev(name, getattr(inp, name), real, grid, dev)
+    _check_dev("r0", inp.r0, real, (N, 3), dev)
+    _check_dev("phi", inp.phi, real, (N,), dev)
+    _check_dev("T2", inp.T2, real, (N,), dev)
+    _check_dev("Mxy", inp.Mxy, cplx, (N, V), dev)
+    _check_dev("M.data", inp.M.data, real, (inp.M.nnz,), dev)
+    _check_dev("out", out, cplx, (*grid, V), dev)
+    a = L.SignalArgs()
+    a.n_nodes, a.n_vencs = N, V
+    a.n_ro, a.n_lines, a.n_kz = grid
+    a.m_rows, a.m_cols = inp.M.shape
+    a.m_nnz = inp.M.nnz
+    a.m_indptr, a.m_indices, a.m_data = _ptr(inp.M.indptr), _ptr(inp.M.indices), _ptr(inp.M.data)
+    a.kx, a.ky, a.kz, a.t = _ptr(inp.kx), _ptr(inp.ky), _ptr(inp.kz), _ptr(inp.t)
+    a.r0, a.phi, a.T2, a.Mxy = _ptr(inp.r0), _ptr(inp.phi), _ptr(inp.T2), _ptr(inp.Mxy)
+    a.motion = C.pointer(motion.struct)
+    a.out = out.data_ptr()
+    return a
+
+
+def signal(inp: SignalInputs, motion: LoweredMotion, precision: str = "f32",
+           out: torch.Tensor | None = None) -> torch.Tensor:
+    """k-space (n_ro, n_lines, n_kz, V) of the mass-weighted NUDFT."""
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+    dev = inp.r0.device
+    cplx = torch.complex128 if precision == "f64" else torch.complex64
+    if out is None:
+        out = torch.empty((*inp.kx.shape, inp.Mxy.shape[1]), dtype=cplx, device=dev)
+    a = signal_args(inp, motion, precision, out)
+    nbytes = C.c_size_t()
+    L.check(L.lib().fm_signal_workspace_size(C.byref(a), PRECISIONS[precision], C.byref(nbytes)))
+    ws = workspace(dev, nbytes.value)
+    L.check(L.lib().fm_signal(ctx_for(dev), C.byref(a), PRECISIONS[precision], ws.data_ptr(), ws.numel()))
+    return out
+
+
+def count_time_runs(t: np.ndarray) -> int:
+    t = np.ascontiguousarray(t).reshape(-1)
+    return int(L.lib().fm_signal_count_time_runs(t.ctypes.data_as(C.c_void_p), t.size,
+                                                 1 if t.dtype == np.float64 else 0))
+
+
+# ------------------------------------------------------------------- Mass --
+
+def _mass_args(elems: torch.Tensor, nodes: torch.Tensor, qweights: torch.Tensor, tab: torch.Tensor) -> L.MassArgs:
+    dev = nodes.device
+    E, nb = elems.shape
+    N = nodes.shape[0]
+    Q = qweights.shape[0]
+    _check_dev("elems", elems, torch.int32, (E, nb), dev)
+    _check_dev("nodes", nodes, nodes.dtype, (N, 3), dev)
+    _check_dev("qweights", qweights, nodes.dtype, (Q,), dev)
+    _check_dev("tabulated", tab, nodes.dtype, (Q, 4, nb), dev)
+    a = L.MassArgs()
+    a.n_elems, a.nodes_per_elem = E, nb
+    a.elems = _ptr(elems)
+    a.n_nodes = N
+    a.nodes = _ptr(nodes)
+    a.n_qpoints = Q
+    a.qweights = _ptr(qweights)
+    a.tabulated = _ptr(tab)
+    return a
+
+
+def mass_assemble(elems, nodes, qweights, tab):
+    """CSC (indptr, indices, data) of the assembled mass matrix."""
+    dev = nodes.device
+    is_double = 1 if nodes.dtype == torch.float64 else 0
+    a = _mass_args(elems, nodes, qweights, tab)
+    nbytes = C.c_size_t()
+    L.check(L.lib().fm_mass_workspace_size(C.byref(a), is_double, C.byref(nbytes)))
+    ws = workspace(dev, nbytes.value)
+    nnz = C.c_int64()
+    N = nodes.shape[0]
+    indptr = torch.empty((N + 1,), dtype=torch.int32, device=dev)
+    ctx = ctx_for(dev)
+    L.check(L.lib().fm_mass_assemble(ctx, C.byref(a), is_double, C.byref(nnz), indptr.data_ptr(), None, None, 0,
+                                     ws.data_ptr(), ws.numel()))
+    indices = torch.empty((nnz.value,), dtype=torch.int32, device=dev)
+    data = torch.empty((nnz.value,), dtype=nodes.dtype, device=dev)
+    L.check(L.lib().fm_mass_assemble(ctx, C.byref(a), is_double, C.byref(nnz), indptr.data_ptr(),
+                                     indices.data_ptr(), data.data_ptr(), nnz.value, ws.data_ptr(), ws.numel()))
+    return indptr, indices, data
+
+
+def mass_lumped(elems, nodes, qweights, tab) -> torch.Tensor:
+    """Row sums of the assembled mass matrix (FEMPhantom.mass_matrix(lumped=True))."""
+    dev = nodes.device
+    is_double = 1 if nodes.dtype == torch.float64 else 0
+    a = _mass_args(elems, nodes, qweights, tab)
+    nbytes = C.c_size_t()
+    L.check(L.lib().fm_mass_workspace_size(C.byref(a), is_double, C.byref(nbytes)))
+    ws = workspace(dev, nbytes.value)
+    out = torch.empty((nodes.shape[0],), dtype=nodes.dtype, device=dev)
+    L.check(L.lib().fm_mass_lumped(ctx_for(dev), C.byref(a), is_double, out.data_ptr(), ws.data_ptr(),
+                                   ws.numel()))
+    return out
