@@ -113,7 +113,7 @@ inline int ctx_ok(const fm_ctx *ctx) {
   return FM_OK;
 }
 
-inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 // Records a start event for a named launch when timing is enabled; returns
 // the slot to pass to timer_stop (or -1).

@@ -40,8 +40,9 @@ def test_static_history_matches_restatement(cuda):
     assert fp64.rel_l2(mg, mo) < 2e-6
     assert fp64.rel_l2(zg, zo) < 1e-6
     m64, z64 = fp64.bloch(r0, T1, T2, dB, 1.0, float(GAMMA), b.rf, b.G, b.dt, Mxy0, Mz0, history=True)
+    # float32 vs float64: the reference's own single-precision error
     assert fp64.rel_l2(mg, m64) < 1e-5
-    assert fp64.rel_l2(zg, z64) < 1e-6
+    assert fp64.rel_l2(zg, z64) < 5e-6
 
 
 def test_pod_motion_lowered_equals_sampled_callable(cuda):

@@ -1,0 +1,106 @@
+"""Split-BF16 tensor-core Signal (precision="bf16x3") against the FP64
+oracle: at most 1e-4 relative L2 on factored Cartesian runs and on generic
+(non-separable) runs, with motion, several column counts and tile edges."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from oracle import fp64
+from feelmri_b200 import workloads as W
+from feelmri_b200.MRI import Signal, signal_call_times
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4  # split-BF16 form against FP64
+
+
+def _case(n=3000, V=4, seed=0):
+    mesh = W.cylinder(n)
+    N = mesh.n_nodes
+    rng = np.random.default_rng(seed)
+    Mxy = ((rng.normal(size=(N, V)) + 1j * rng.normal(size=(N, V))) * 0.1).astype(np.complex64)
+    phi = W.off_resonance(N)
+    _, T2 = W.tissue(N, seed)
+    M = sp.lil_matrix((N, N))
+    M.setdiag(rng.uniform(1e-7, 3e-7, N))
+    return mesh, N, M, Mxy, phi, T2
+
+
+def _ref(M, traj, r0, phi, T2, Mxy, pod=None, idx=None):
+    disp = None
+    if pod is not None:
+        disp = np.stack([pod(t) for t in signal_call_times(traj.t)[1:]])
+    return fp64.signal(sp.csc_matrix(M), *traj.points, traj.t, r0, phi, T2, Mxy, disp=disp, pi_mode="float",
+                       sample_idx=idx)
+
+
+def test_factored_cartesian_static(cuda):
+    mesh, N, M, Mxy, phi, T2 = _case()
+    traj = W.cartesian(res=(12, 24, 8))
+    r0 = mesh.nodes.astype(np.float32)
+    K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    assert K.dtype == np.complex64 and K.shape == (*traj.shape, 4)
+    err = fp64.rel_l2(K, _ref(M, traj, r0, phi, T2, Mxy))
+    assert err < TOL, err
+
+
+def test_factored_cartesian_with_flow(cuda):
+    mesh, N, M, Mxy, phi, T2 = _case(n=5000)
+    traj = W.cartesian(res=(16, 40, 32), fov=(0.1, 0.1, 0.1))
+    r0 = mesh.nodes.astype(np.float32)
+    vel = W.poiseuille_velocity(mesh.nodes, radius=0.04, period=60.0, n_frames=6)
+    vel.update_timeshift(11.0)
+    K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, vel, precision="bf16x3")
+    err = fp64.rel_l2(K, _ref(M, traj, r0, phi, T2, Mxy, pod=vel))
+    assert err < TOL, err
+    K32 = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, vel)
+    assert fp64.rel_l2(K, K32) < TOL
+
+
+def test_generic_radial_runs(cuda):
+    mesh, N, M, Mxy, phi, T2 = _case(n=2500, V=8)
+    traj = W.radial3d(n_ro=12, n_spokes=300, kmax=500.0)
+    r0 = mesh.nodes.astype(np.float32)
+    pod = W.sinusoidal_pod(N, n_modes=3, amp=1e-3, period=50.0, n_frames=8)
+    K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, pod, precision="bf16x3")
+    err = fp64.rel_l2(K, _ref(M, traj, r0, phi, T2, Mxy, pod=pod))
+    assert err < TOL, err
+
+
+@pytest.mark.parametrize("V", [1, 3, 17])
+def test_column_groups_and_tiles(cuda, V):
+    mesh, N, M, Mxy, phi, T2 = _case(n=1500, V=V)
+    traj = W.cartesian(res=(4, 140, 6))  # 140 lines: two row tiles
+    r0 = mesh.nodes.astype(np.float32)
+    K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    err = fp64.rel_l2(K, _ref(M, traj, r0, phi, T2, Mxy))
+    assert err < TOL, err
+
+
+def test_many_kz_columns_and_spiral(cuda):
+    mesh, N, M, Mxy, phi, T2 = _case(n=1200, V=4)
+    traj = W.cartesian(res=(3, 8, 70))  # 70 kz values: several column tiles
+    r0 = mesh.nodes.astype(np.float32)
+    K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    assert fp64.rel_l2(K, _ref(M, traj, r0, phi, T2, Mxy)) < TOL
+    sp_traj = W.spiral_stack(n_ro=64, n_interleaves=4, n_kz=4)
+    K = Signal(0, M, sp_traj.points, sp_traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    assert fp64.rel_l2(K, _ref(M, sp_traj, r0, phi, T2, Mxy)) < TOL
+
+
+def test_deterministic_and_edge_cases(cuda):
+    mesh, N, M, Mxy, phi, T2 = _case(n=800, V=2)
+    traj = W.cartesian(res=(5, 6, 3))
+    r0 = mesh.nodes.astype(np.float32)
+    a = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    b = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    np.testing.assert_array_equal(a, b)
+    t = traj.t.copy()
+    t[1, 2, 1] = np.nan
+    K = Signal(0, M, traj.points, t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    bad = ~np.isfinite(K)
+    assert bad[1, 2, 1].all()
+    with pytest.raises(TypeError):
+        d = np.float64
+        Signal(0, M, [p.astype(d) for p in traj.points], traj.t.astype(d), mesh.nodes, phi.astype(d), T2.astype(d),
+               Mxy.astype(np.complex128), None, precision="bf16x3")
