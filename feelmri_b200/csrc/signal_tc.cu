@@ -19,13 +19,19 @@
 // * Phases.  k . r is evaluated in FP64 and reduced modulo one cycle before
 //   the FP32 sin/cos, so far nodes at high k keep their digits.
 //
-// Block: warps 0-3 produce operand tiles (16 nodes per pipeline stage, 4
-// stages of shared memory in the UMMA no-swizzle K-major layout) and run the
-// epilogue; warp 4 owns the tensor memory and one of its threads issues the
-// MMAs.  Stages are handed over with mbarriers; tcgen05.commit frees a stage
-// when the MMAs that read it have completed.  All waits are bounded: on
-// timeout the block records an error, drains and frees its tensor memory.
+// Block (persistent, one per SM): warps 0-7 produce operand tiles (16 nodes
+// per pipeline stage, 4 stages of shared memory in the UMMA no-swizzle
+// K-major layout) and drain the accumulators; one thread of warp 8 issues the
+// MMAs and warp 8 owns the tensor memory.  Stages are handed over with
+// mbarriers; tcgen05.commit frees a stage when the MMAs that read it have
+// completed.  The tensor core's FP32 accumulation truncates, so each
+// accumulator only collects 32 stages: two accumulators alternate in tensor
+// memory and the producers drain the idle one into an FP32 (round-to-nearest)
+// running sum.  Blocks loop over work units (row/column tile of a run x node
+// range).  All waits are bounded: on timeout the block records an error,
+// lets its MMAs finish and frees its tensor memory.
 #include <cuda_bf16.h>
+#include <cmath>
 #include <cub/cub.cuh>
 
 #include "signal_common.cuh"
@@ -37,9 +43,15 @@ constexpr int kTcRows = 128;        // UMMA M
 constexpr int kTcNodes = 16;        // nodes per stage -> K = 32 (two UMMA K steps)
 constexpr int kTcStages = 4;
 constexpr int kTcBlockNodes = 128;  // nodes whose per-run data is formed together
-constexpr int kTcProducers = 128;
-constexpr int kTcThreads = 160;
+constexpr int kTcProducers = 256;   // warps 0-7
+constexpr int kTcMmaWarp = 8;
+constexpr int kTcThreads = 288;
 constexpr int kTcVGroup = 16;       // Mxy columns per launch
+// Stages accumulated in one tensor-memory accumulator before it is drained
+// into an FP32 round-to-nearest running sum.  The tensor core's FP32
+// accumulation truncates, so its error grows with the number of MMAs added
+// into one accumulator; 32 stages (512 nodes, 192 MMAs) keep it near 1e-5.
+constexpr int kTcDrain = 32;
 constexpr uint64_t kTcWaitNs = 2000000000ull;
 constexpr uint32_t kAStageBytes = kTcRows * 2 * kTcNodes * 2;  // 128 rows x 32 K x bf16 = 8 KB
 
@@ -63,11 +75,12 @@ struct TcDev {
   const double *run_t;
   const TcRun *runs;
   const TcItem *items;
-  int item0;
-  int Qt, NT, tmem_cols;
+  int item0, n_items;
+  int Qt, NT, acc_cols;
   int splits;
   int64_t chunk;
   float2 *out;
+  float *scratch;  // per block: 128 x NT running sums
   int *error;
 };
 
@@ -127,6 +140,11 @@ __device__ inline void store_split8(uint32_t hi_addr, uint32_t lo_addr, const fl
   ptx::st_shared_v4(lo_addr, l[0], l[1], l[2], l[3]);
 }
 
+__device__ inline void store_zero8(uint32_t hi_addr, uint32_t lo_addr) {
+  ptx::st_shared_v4(hi_addr, 0u, 0u, 0u, 0u);
+  ptx::st_shared_v4(lo_addr, 0u, 0u, 0u, 0u);
+}
+
 // exp(-2 pi i c) for c in cycles given in FP64: reduce modulo one, then FP32.
 __device__ inline float2 cis_neg_cycles(double c) {
   const double f = c - rint(c);
@@ -135,12 +153,14 @@ __device__ inline float2 cis_neg_cycles(double c) {
   return make_float2(co, -s);
 }
 
+// OR of a predicate over the 256 producer threads (named barrier 1): used
+// for every decision that must be uniform across them.
 __device__ inline bool producers_any(bool x) {
   uint32_t out;
   asm volatile(
       "{\n\t.reg .pred pi, po;\n\t"
       "setp.ne.u32 pi, %1, 0;\n\t"
-      "bar.red.or.pred po, 1, 128, pi;\n\t"
+      "bar.red.or.pred po, 1, 256, pi;\n\t"
       "selp.u32 %0, 1, 0, po;\n\t}"
       : "=r"(out)
       : "r"((uint32_t)x)
@@ -148,14 +168,96 @@ __device__ inline bool producers_any(bool x) {
   return out != 0;
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p) {
+struct TcUnit {
+  TcItem it;
+  TcRun run;
+  int split, P_tile, Q_tile, n_stages, n_groups;
+  int64_t n_begin, n_end;
+};
+
+__device__ inline TcUnit tc_unit(const TcDev &p, int u) {
+  TcUnit U;
+  const int item = u % p.n_items;
+  U.split = u / p.n_items;
+  U.it = p.items[p.item0 + item];
+  U.run = p.runs[U.it.run];
+  U.P_tile = min(kTcRows, U.run.P - U.it.p0);
+  U.Q_tile = min(p.Qt, U.run.Q - U.it.q0);
+  U.n_begin = (int64_t)U.split * p.chunk;
+  U.n_end = min(p.N, U.n_begin + p.chunk);
+  U.n_stages = U.n_end > U.n_begin ? (int)ceil_div(U.n_end - U.n_begin, kTcNodes) : 0;
+  U.n_groups = (int)ceil_div(U.n_stages, kTcDrain);
+  return U;
+}
+
+// Adds accumulator `buf` (one drained group) into the block's running sums,
+// or, for the unit's last group, writes running sums + accumulator to the
+// output samples.  Executed by all 256 producers: warp w reads TMEM lanes of
+// quarter w % 4 and column half w / 4.
+__device__ inline bool tc_drain(const TcDev &p, const TcUnit &U, uint64_t *accfull, uint64_t *accfree, uint32_t tmem,
+                                int gg, bool first, bool final, bool ok_in) {
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int b = gg & 1;
+  const bool waited = ptx::mbar_wait(&accfull[b], (gg >> 1) & 1, kTcWaitNs);
+  const bool ok = ok_in && !producers_any(!waited);
+  ptx::tc_fence_after();
+  const int quarter = warp & 3, half = warp >> 2;
+  const int row = quarter * 32 + (tid & 31);
+  const int cph = ((p.NT / 2 + 15) / 16) * 16;
+  const int c_begin = half * cph, c_end = min(p.NT, c_begin + cph);
+  float *srow = p.scratch + ((size_t)blockIdx.x * kTcRows + row) * p.NT;
+  const bool row_ok = row < U.P_tile;
+  float2 *dst = p.out + (int64_t)U.split * p.S * p.V;
+  const int s_row = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz + U.it.q0 : U.it.p0 + row);
+  for (int c0 = c_begin; c0 < c_end; c0 += 16) {
+    uint32_t r[16];
+    if (ok) {
+      ptx::tmem_ld16(tmem + (uint32_t)(b * p.acc_cols) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, r);
+      ptx::tmem_wait_ld();
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) r[i] = 0u;
+    }
+    if (!row_ok) continue;
+    float v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+    if (!first) {
+      const float4 *src = reinterpret_cast<const float4 *>(srow + c0);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float4 a = src[i];
+        v[4 * i] += a.x; v[4 * i + 1] += a.y; v[4 * i + 2] += a.z; v[4 * i + 3] += a.w;
+      }
+    }
+    if (!final) {
+      float4 *d4 = reinterpret_cast<float4 *>(srow + c0);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) d4[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int jj = (c0 >> 1) + i;
+        const int q = jj / p.VG, vv = jj % p.VG;
+        if (q < U.Q_tile) dst[(int64_t)(s_row + q) * p.V + p.v0 + vv] = make_float2(v[2 * i], v[2 * i + 1]);
+      }
+    }
+  }
+  ptx::tc_fence_before();
+  ptx::mbar_arrive(&accfree[b]);
+  return ok;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n_units) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
   const TcSmem L = tc_smem_layout(p.NT, p.VG, p.Qt);
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + L.bars);
   uint64_t *empty = full + kTcStages;
-  uint64_t *accum = empty + kTcStages;
+  uint64_t *accfull = empty + kTcStages;
+  uint64_t *accfree = accfull + 2;
+  uint64_t *done = accfree + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L.misc);
   float4 *pos = reinterpret_cast<float4 *>(smem + L.pos);
   float2 *wblk = reinterpret_cast<float2 *>(smem + L.w);
@@ -163,38 +265,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p) {
   double *kq = reinterpret_cast<double *>(smem + L.kq);
   const uint32_t sbase = ptx::smem_addr(smem);
 
-  const TcItem it = p.items[p.item0 + blockIdx.x];
-  const TcRun run = p.runs[it.run];
-  const int split = blockIdx.y;
-  const int P_tile = min(kTcRows, run.P - it.p0);
-  const int Q_tile = min(p.Qt, run.Q - it.q0);
-  const int64_t n_begin = (int64_t)split * p.chunk;
-  const int64_t n_end = min(p.N, n_begin + p.chunk);
-  const int n_stages = n_end > n_begin ? (int)ceil_div(n_end - n_begin, kTcNodes) : 0;
-  const double tg_d = p.run_t[it.run];
-  const float tg = (float)tg_d;
-
-  // ---- set-up: zero operand ring, barriers, tensor memory, k vectors ----
-  for (uint32_t o = tid * 16; o < kTcStages * L.stage_bytes; o += kTcThreads * 16)
-    ptx::st_shared_v4(sbase + o, 0u, 0u, 0u, 0u);
   if (tid == 0) {
     for (int s = 0; s < kTcStages; ++s) {
       ptx::mbar_init(&full[s], kTcProducers);
       ptx::mbar_init(&empty[s], 1);
     }
-    ptx::mbar_init(accum, 1);
-    tmem_slot[1] = 0;  // abort flag of the MMA thread
+    for (int b = 0; b < 2; ++b) {
+      ptx::mbar_init(&accfull[b], 1);
+      ptx::mbar_init(&accfree[b], kTcProducers);
+    }
+    ptx::mbar_init(done, 1);
     ptx::fence_mbar_init();
   }
-  if (warp == 4) ptx::tmem_alloc(tmem_slot, p.tmem_cols);
-  // kq_q = k(start + q) - k(start) for the columns of this tile (factored)
-  for (int q = tid; q < Q_tile; q += kTcThreads) {
-    const int s_q = run.start + it.q0 + q, s_0 = run.start;
-    kq[3 * q + 0] = run.factored ? (double)p.kx[s_q] - (double)p.kx[s_0] : 0.0;
-    kq[3 * q + 1] = run.factored ? (double)p.ky[s_q] - (double)p.ky[s_0] : 0.0;
-    kq[3 * q + 2] = run.factored ? (double)p.kz[s_q] - (double)p.kz[s_0] : 0.0;
-  }
-  ptx::fence_proxy_async_smem();
+  if (warp == kTcMmaWarp) ptx::tmem_alloc(tmem_slot, 2 * p.acc_cols);
   ptx::tc_fence_before();
   __syncthreads();
   ptx::tc_fence_after();
@@ -202,183 +285,207 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p) {
   const uint32_t idesc = ptx::idesc_bf16_f32(kTcRows, p.NT);
   bool ok = true;
 
-  if (warp < 4) {
+  if (warp < kTcMmaWarp) {
     // ------------------------------------------------------ producers --
-    const int prow = tid;  // A row handled by this thread
-    double kpx = 0, kpy = 0, kpz = 0;
-    const bool a_active = prow < P_tile;
-    if (a_active) {
-      const int s_p = run.start + (run.factored ? (it.p0 + prow) * p.n_kz : it.p0 + prow);
-      kpx = p.kx[s_p];
-      kpy = p.ky[s_p];
-      kpz = p.kz[s_p];
-    }
-    const int bj = tid;  // (q, v) pair handled by this thread for B
-    const bool b_active = bj < Q_tile * p.VG;
-    const int bq = b_active ? bj / p.VG : 0, bv = b_active ? bj % p.VG : 0;
-    const float *wrun = p.weights ? p.weights + (int64_t)it.run * p.md.slots : nullptr;
-
-    for (int st = 0; st < n_stages; ++st) {
-      const int s = st % kTcStages;
-      const uint32_t round = st / kTcStages;
-      const int j = st % (kTcBlockNodes / kTcNodes);
-      if (j == 0) {
-        // per-run node data for the next 128 nodes
-        ptx::named_barrier(1, kTcProducers);
-        const int64_t n = n_begin + (int64_t)st * kTcNodes + tid;
-        float4 pp = make_float4(0.f, 0.f, 0.f, 0.f);
-        float2 wv[kTcVGroup];
-#pragma unroll
-        for (int v = 0; v < kTcVGroup; ++v) wv[v] = make_float2(0.f, 0.f);
-        if (n < n_end) {
-          float x = p.r0[3 * n + 0], y = p.r0[3 * n + 1], z = p.r0[3 * n + 2];
-          if (p.md.kind == FM_MOTION_TERMS) {
-            float dx, dy, dz;
-            motion_disp(p.md, wrun, n, p.N, dx, dy, dz);
-            x = x + dx; y = y + dy; z = z + dz;
-          } else if (p.table) {
-            const float *d = p.table + ((int64_t)it.run * p.N + n) * 3;
-            x = x + d[0]; y = y + d[1]; z = z + d[2];
-          }
-          pp = make_float4(x, y, z, 1.f);
-          const float decay = expf(-tg * (1.0f / p.T2[n]));
-          float so, co;
-          sincosf(p.phi[n] * tg, &so, &co);
-          const float er = decay * co, ei = decay * so;
-          for (int v = 0; v < p.VG; ++v) {
-            const float2 m = p.MM[n * p.V + p.v0 + v];
-            wv[v] = make_float2(m.x * er - m.y * ei, m.x * ei + m.y * er);
-          }
-        }
-        pos[tid] = pp;
-        for (int v = 0; v < p.VG; ++v) wblk[tid * p.VG + v] = wv[v];
-        ptx::named_barrier(1, kTcProducers);
+    const int row = tid & (kTcRows - 1);  // A row / B (q, v) pair of this thread
+    const int half = tid >> 7;            // which 8 of the 16 nodes of a stage
+    int gst = 0, gbase = 0;
+    for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
+      const TcUnit U = tc_unit(p, u);
+      ptx::named_barrier(1, kTcProducers);  // previous unit's readers of kq are done
+      for (int q = tid; q < U.Q_tile; q += kTcProducers) {
+        const int s_q = U.run.start + U.it.q0 + q, s_0 = U.run.start;
+        kq[3 * q + 0] = U.run.factored ? (double)p.kx[s_q] - (double)p.kx[s_0] : 0.0;
+        kq[3 * q + 1] = U.run.factored ? (double)p.ky[s_q] - (double)p.ky[s_0] : 0.0;
+        kq[3 * q + 2] = U.run.factored ? (double)p.kz[s_q] - (double)p.kz[s_0] : 0.0;
       }
-      // wait until the MMAs that last read stage s are done
-      const bool waited = ptx::mbar_wait(&empty[s], (round & 1) ^ 1, kTcWaitNs);
-      if (producers_any(!waited)) {
-        ok = false;
-        break;
-      }
-      const float4 *pn = pos + j * kTcNodes;
-      const float2 *wn = wblk + j * kTcNodes * p.VG;
-      // e_q(n) = exp(-2 pi i kq_q . r_n) for this stage's nodes
-      for (int idx = tid; idx < Q_tile * kTcNodes; idx += kTcProducers) {
-        const int q = idx / kTcNodes, n = idx % kTcNodes;
-        const float4 r = pn[n];
-        float2 e = make_float2(1.f, 0.f);
-        if (run.factored) {
-          const double c = kq[3 * q] * (double)r.x + kq[3 * q + 1] * (double)r.y + kq[3 * q + 2] * (double)r.z;
-          e = cis_neg_cycles(c);
-        }
-        etab[idx] = e;
-      }
-      ptx::named_barrier(1, kTcProducers);
-      const uint32_t stage = sbase + s * L.stage_bytes;
+      const bool a_active = row < U.P_tile;
+      double kpx = 0, kpy = 0, kpz = 0;
       if (a_active) {
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {  // 4 chunks of 4 nodes (8 K values)
-          float x[8];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const float4 r = pn[4 * h + u];
-            const double c = kpx * (double)r.x + kpy * (double)r.y + kpz * (double)r.z;
-            float2 e = cis_neg_cycles(c);
-            if (r.w == 0.f) e = make_float2(0.f, 0.f);
-            x[2 * u] = e.x;
-            x[2 * u + 1] = e.y;
-          }
-          const uint32_t off = kmajor_offset(prow, 8 * h, kTcRows);
-          store_split8(stage + L.a_hi + off, stage + L.a_lo + off, x);
-        }
+        const int s_p = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz : U.it.p0 + row);
+        kpx = p.kx[s_p];
+        kpy = p.ky[s_p];
+        kpz = p.kz[s_p];
       }
-      if (b_active) {
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          float xr[8], xi[8];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int n = 4 * h + u;
-            const float2 e = etab[bq * kTcNodes + n];
-            const float2 w = wn[n * p.VG + bv];
-            const float br = e.x * w.x - e.y * w.y, bi = e.x * w.y + e.y * w.x;
-            xr[2 * u] = br;
-            xr[2 * u + 1] = -bi;
-            xi[2 * u] = bi;
-            xi[2 * u + 1] = br;
-          }
-          const uint32_t o_re = kmajor_offset(2 * bj, 8 * h, p.NT);
-          const uint32_t o_im = kmajor_offset(2 * bj + 1, 8 * h, p.NT);
-          store_split8(stage + L.b_hi + o_re, stage + L.b_lo + o_re, xr);
-          store_split8(stage + L.b_hi + o_im, stage + L.b_lo + o_im, xi);
-        }
-      }
-      ptx::fence_proxy_async_smem();
-      ptx::mbar_arrive(&full[s]);
-    }
-  } else if (tid == 4 * 32) {
-    // ------------------------------------------------------ MMA issue --
-    for (int st = 0; st < n_stages; ++st) {
-      const int s = st % kTcStages;
-      const uint32_t round = st / kTcStages;
-      if (!ptx::mbar_wait(&full[s], round & 1, kTcWaitNs)) {
-        ok = false;
-        break;
-      }
-      ptx::tc_fence_after();
-      const uint32_t stage = sbase + s * L.stage_bytes;
-#pragma unroll
-      for (int ks = 0; ks < 2; ++ks) {
-        const uint64_t ah = ptx::smem_desc(stage + L.a_hi + ks * kTcRows * 32, 128, 256);
-        const uint64_t al = ptx::smem_desc(stage + L.a_lo + ks * kTcRows * 32, 128, 256);
-        const uint64_t bh = ptx::smem_desc(stage + L.b_hi + ks * p.NT * 32, 128, 256);
-        const uint64_t bl = ptx::smem_desc(stage + L.b_lo + ks * p.NT * 32, 128, 256);
-        ptx::mma_bf16(tmem, ah, bh, idesc, (st > 0 || ks > 0) ? 1u : 0u);
-        ptx::mma_bf16(tmem, ah, bl, idesc, 1u);
-        ptx::mma_bf16(tmem, al, bh, idesc, 1u);
-      }
-      ptx::mma_commit(&empty[s]);
-    }
-    ptx::mma_commit(accum);
-    if (!ok) tmem_slot[1] = 1;
-  }
+      const bool b_rows = 2 * row < p.NT;
+      const bool b_active = row < U.Q_tile * p.VG;
+      const int bq = b_active ? row / p.VG : 0, bv = b_active ? row % p.VG : 0;
+      const float *wrun = p.weights ? p.weights + (int64_t)U.it.run * p.md.slots : nullptr;
+      const float tg = (float)p.run_t[U.it.run];
+      int next_drain = 0;
 
-  // ---------------------------------------------------------- epilogue --
-  if (warp < 4) {
-    const bool done = ptx::mbar_wait(accum, 0, kTcWaitNs);
-    ptx::tc_fence_after();
-    if (!done || !ok) atomicExch(p.error, 1);
-    const int prow = warp * 32 + (tid & 31);
-    float2 *dst = p.out + (int64_t)split * p.S * p.V;
-    const bool row_ok = prow < P_tile;
-    const int s_row = run.start + (run.factored ? (it.p0 + prow) * p.n_kz + it.q0 : it.p0 + prow);
-    for (int c0 = 0; c0 < p.NT; c0 += 16) {
-      uint32_t r[16];
-      if (n_stages > 0 && done) {
-        ptx::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
-        ptx::tmem_wait_ld();
-      } else {
+      for (int st = 0; st < U.n_stages; ++st, ++gst) {
+        const int s = gst % kTcStages;
+        const uint32_t round = gst / kTcStages;
+        const int j = st % (kTcBlockNodes / kTcNodes);
+        if (j == 0) {
+          ptx::named_barrier(1, kTcProducers);
+          if (tid < kTcBlockNodes) {
+            const int64_t n = U.n_begin + (int64_t)st * kTcNodes + tid;
+            float4 pp = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (n < U.n_end) {
+              float x = p.r0[3 * n + 0], y = p.r0[3 * n + 1], z = p.r0[3 * n + 2];
+              if (p.md.kind == FM_MOTION_TERMS) {
+                float dx, dy, dz;
+                motion_disp(p.md, wrun, n, p.N, dx, dy, dz);
+                x = x + dx; y = y + dy; z = z + dz;
+              } else if (p.table) {
+                const float *d = p.table + ((int64_t)U.it.run * p.N + n) * 3;
+                x = x + d[0]; y = y + d[1]; z = z + d[2];
+              }
+              pp = make_float4(x, y, z, 1.f);
+              const float decay = expf(-tg * (1.0f / p.T2[n]));
+              float so, co;
+              sincosf(p.phi[n] * tg, &so, &co);
+              const float er = decay * co, ei = decay * so;
+              for (int v = 0; v < p.VG; ++v) {
+                const float2 m = p.MM[n * p.V + p.v0 + v];
+                wblk[tid * p.VG + v] = make_float2(m.x * er - m.y * ei, m.x * ei + m.y * er);
+              }
+            } else {
+              for (int v = 0; v < p.VG; ++v) wblk[tid * p.VG + v] = make_float2(0.f, 0.f);
+            }
+            pos[tid] = pp;
+          }
+          ptx::named_barrier(1, kTcProducers);
+        }
+        // wait until the MMAs that last read stage s are done
+        const bool waited = ptx::mbar_wait(&empty[s], (round & 1) ^ 1, kTcWaitNs);
+        if (producers_any(!waited)) {
+          ok = false;
+          break;
+        }
+        const float4 *pn = pos + j * kTcNodes;
+        const float2 *wn = wblk + j * kTcNodes * p.VG;
+        for (int idx = tid; idx < U.Q_tile * kTcNodes; idx += kTcProducers) {
+          const int q = idx / kTcNodes, n = idx % kTcNodes;
+          const float4 r = pn[n];
+          float2 e = make_float2(1.f, 0.f);
+          if (U.run.factored) {
+            const double c = kq[3 * q] * (double)r.x + kq[3 * q + 1] * (double)r.y + kq[3 * q + 2] * (double)r.z;
+            e = cis_neg_cycles(c);
+          }
+          etab[idx] = e;
+        }
+        ptx::named_barrier(1, kTcProducers);
+        const uint32_t stage = sbase + s * L.stage_bytes;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) r[i] = 0u;
-      }
-      if (!row_ok) continue;
+        for (int hh = 0; hh < 2; ++hh) {  // two chunks of 4 nodes (8 K values)
+          const int h = 2 * half + hh;
+          const uint32_t off = kmajor_offset(row, 8 * h, kTcRows);
+          if (a_active) {
+            float x[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int jj = (c0 >> 1) + i;
-        const int q = jj / p.VG, v = jj % p.VG;
-        if (q < Q_tile) {
-          dst[(int64_t)(s_row + q) * p.V + p.v0 + v] = make_float2(__uint_as_float(r[2 * i]),
-                                                                   __uint_as_float(r[2 * i + 1]));
+            for (int u4 = 0; u4 < 4; ++u4) {
+              const float4 r = pn[4 * h + u4];
+              const double c = kpx * (double)r.x + kpy * (double)r.y + kpz * (double)r.z;
+              float2 e = cis_neg_cycles(c);
+              if (r.w == 0.f) e = make_float2(0.f, 0.f);
+              x[2 * u4] = e.x;
+              x[2 * u4 + 1] = e.y;
+            }
+            store_split8(stage + L.a_hi + off, stage + L.a_lo + off, x);
+          } else {
+            store_zero8(stage + L.a_hi + off, stage + L.a_lo + off);
+          }
+          if (b_rows) {
+            const uint32_t o_re = kmajor_offset(2 * row, 8 * h, p.NT);
+            const uint32_t o_im = kmajor_offset(2 * row + 1, 8 * h, p.NT);
+            if (b_active) {
+              float xr[8], xi[8];
+#pragma unroll
+              for (int u4 = 0; u4 < 4; ++u4) {
+                const int n = 4 * h + u4;
+                const float2 e = etab[bq * kTcNodes + n];
+                const float2 w = wn[n * p.VG + bv];
+                const float br = e.x * w.x - e.y * w.y, bi = e.x * w.y + e.y * w.x;
+                xr[2 * u4] = br;
+                xr[2 * u4 + 1] = -bi;
+                xi[2 * u4] = bi;
+                xi[2 * u4 + 1] = br;
+              }
+              store_split8(stage + L.b_hi + o_re, stage + L.b_lo + o_re, xr);
+              store_split8(stage + L.b_hi + o_im, stage + L.b_lo + o_im, xi);
+            } else {
+              store_zero8(stage + L.b_hi + o_re, stage + L.b_lo + o_re);
+              store_zero8(stage + L.b_hi + o_im, stage + L.b_lo + o_im);
+            }
+          }
+        }
+        ptx::fence_proxy_async_smem();
+        ptx::mbar_arrive(&full[s]);
+        // drain the previous group a few stages into the current one, when the
+        // MMAs that wrote it have (almost surely) completed
+        if (st % kTcDrain == kTcStages - 1 && st / kTcDrain >= 1 && next_drain == st / kTcDrain - 1) {
+          ok = tc_drain(p, U, accfull, accfree, tmem, gbase + next_drain, next_drain == 0, false, ok);
+          ++next_drain;
+          if (!ok) break;
         }
       }
+      while (ok && next_drain < U.n_groups) {
+        ok = tc_drain(p, U, accfull, accfree, tmem, gbase + next_drain, next_drain == 0,
+                      next_drain == U.n_groups - 1, ok);
+        ++next_drain;
+      }
+      if (ok && U.n_groups == 0 && row == tid) {
+        // no nodes in this split: its share of the tile is zero
+        float2 *dst = p.out + (int64_t)U.split * p.S * p.V;
+        if (row < U.P_tile) {
+          const int s_row = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz + U.it.q0 : U.it.p0 + row);
+          for (int q = 0; q < U.Q_tile; ++q)
+            for (int v = 0; v < p.VG; ++v) dst[(int64_t)(s_row + q) * p.V + p.v0 + v] = make_float2(0.f, 0.f);
+        }
+      }
+      gbase += U.n_groups;
     }
+    if (!ok) atomicExch(p.error, 1);
+  } else if (tid == kTcMmaWarp * 32) {
+    // ------------------------------------------------------ MMA issue --
+    int gst = 0, gbase = 0;
+    for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
+      const TcUnit U = tc_unit(p, u);
+      for (int st = 0; st < U.n_stages; ++st, ++gst) {
+        const int s = gst % kTcStages;
+        const uint32_t round = gst / kTcStages;
+        const int gg = gbase + st / kTcDrain;
+        const int b = gg & 1;
+        const bool group_start = (st % kTcDrain) == 0;
+        if (group_start && gg >= 2 && !ptx::mbar_wait(&accfree[b], ((gg - 2) >> 1) & 1, kTcWaitNs)) {
+          ok = false;
+          break;
+        }
+        if (!ptx::mbar_wait(&full[s], round & 1, kTcWaitNs)) {
+          ok = false;
+          break;
+        }
+        ptx::tc_fence_after();
+        const uint32_t stage = sbase + s * L.stage_bytes;
+        const uint32_t acc = tmem + (uint32_t)(b * p.acc_cols);
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+          const uint64_t ah = ptx::smem_desc(stage + L.a_hi + ks * kTcRows * 32, 128, 256);
+          const uint64_t al = ptx::smem_desc(stage + L.a_lo + ks * kTcRows * 32, 128, 256);
+          const uint64_t bh = ptx::smem_desc(stage + L.b_hi + ks * p.NT * 32, 128, 256);
+          const uint64_t bl = ptx::smem_desc(stage + L.b_lo + ks * p.NT * 32, 128, 256);
+          ptx::mma_bf16(acc, ah, bh, idesc, (group_start && ks == 0) ? 0u : 1u);
+          ptx::mma_bf16(acc, ah, bl, idesc, 1u);
+          ptx::mma_bf16(acc, al, bh, idesc, 1u);
+        }
+        ptx::mma_commit(&empty[s]);
+        if ((st % kTcDrain) == kTcDrain - 1 || st == U.n_stages - 1) ptx::mma_commit(&accfull[b]);
+      }
+      gbase += U.n_groups;
+    }
+    // all issued MMAs complete before the tensor memory is released
+    ptx::mma_commit(done);
+    if (!ptx::mbar_wait(done, 0, kTcWaitNs)) ok = false;
+    if (!ok) atomicExch(p.error, 2);
   }
   ptx::tc_fence_before();
   __syncthreads();
-  if (warp == 4) {
+  if (warp == kTcMmaWarp) {
     ptx::tc_fence_after();
-    if (tid == 4 * 32 && tmem_slot[1]) atomicExch(p.error, 2);
-    ptx::tmem_dealloc(tmem, p.tmem_cols);
+    ptx::tmem_dealloc(tmem, 2 * p.acc_cols);
   }
 }
 
@@ -484,6 +591,7 @@ struct TcPlan {
   TcItem *items;
   int *nf, *ng, *of, *og;
   int *error;
+  float *scratch;
   float2 *partials;
   int max_splits;
 };
@@ -509,6 +617,7 @@ static void carve_tc(Carve &c, const fm_signal_args *a, TcPlan &pl) {
   pl.of = c.take<int>(S + 2);
   pl.og = c.take<int>(S + 2);
   pl.error = c.take<int>(4);
+  pl.scratch = c.take<float>((size_t)kSmCount * kTcRows * 256);
   pl.max_splits = tc_max_splits(S, V);
   pl.partials = c.take<float2>((size_t)pl.max_splits * S * V);
 }
@@ -520,20 +629,20 @@ size_t tc_workspace(const fm_signal_args *a) {
   return c.used;
 }
 
-// Splits of the node range: enough blocks to cover the SMs a few times with
-// little tail, each split at least 2048 nodes.
+// Node-range splits: enough work units that the persistent blocks finish
+// together (units per block close to an integer), each split at least 2048
+// nodes; fewer splits win ties.
 static int tc_choose_splits(int64_t items, int64_t N, int max_splits) {
   if (items <= 0) return 1;
   int best = 1;
-  double best_cost = 1e30;
+  double best_eff = -1.0;
   for (int s = 1; s <= max_splits; ++s) {
     if (s > 1 && ceil_div(N, s) < 2048) break;
-    const int64_t blocks = items * s;
-    const int64_t waves = ceil_div(blocks, kSmCount);
-    // time ~ waves x (work per block) ; work per block ~ 1/s
-    const double cost = (double)waves / s + (blocks < kSmCount ? 1.0 : 0.0) * 0.0;
-    if (cost < best_cost - 1e-9) {
-      best_cost = cost;
+    const double units = (double)items * s;
+    const double per_block = units / kSmCount;
+    const double eff = per_block / std::ceil(per_block) * (units < kSmCount ? units / kSmCount : 1.0);
+    if (eff > best_eff + 0.02) {
+      best_eff = eff;
       best = s;
     }
   }
@@ -614,25 +723,27 @@ int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
     p.splits = splits;
     p.chunk = ceil_div(ceil_div(N, splits), kTcNodes) * kTcNodes;
     p.out = (splits > 1) ? pl.partials : out;
+    p.scratch = pl.scratch;
     p.error = pl.error;
-    if (splits > 1) FM_CUDA(cudaMemsetAsync(pl.partials, 0, (size_t)splits * S * V * sizeof(float2), st));
 
     ScopedTimer timer(ctx, "signal_tc");
     for (int kind = 0; kind < 2; ++kind) {
       const int count = kind == 0 ? n_fact : n_gen;
       if (count == 0) continue;
       p.item0 = kind == 0 ? 0 : n_fact;
+      p.n_items = count;
       p.Qt = kind == 0 ? Qt_f : 1;
       const int cols = 2 * p.Qt * VG;
       p.NT = (int)ceil_div(cols, 16) * 16;
-      p.tmem_cols = 32;
-      while (p.tmem_cols < p.NT) p.tmem_cols <<= 1;
+      p.acc_cols = 32;
+      while (p.acc_cols < p.NT) p.acc_cols <<= 1;
       const TcSmem Ls = tc_smem_layout(p.NT, VG, p.Qt);
       const size_t smem = Ls.total + 1024;
       FM_REQUIRE(smem <= 232448, FM_ERR_UNSUPPORTED, "%s: tile needs %zu bytes of shared memory", who, smem);
       FM_CUDA(cudaFuncSetAttribute(signal_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      dim3 grid((unsigned)count, (unsigned)splits);
-      signal_tc_kernel<<<grid, kTcThreads, smem, st>>>(p);
+      const int n_units = count * splits;
+      const int grid = n_units < kSmCount ? n_units : kSmCount;
+      signal_tc_kernel<<<grid, kTcThreads, smem, st>>>(p, n_units);
       count_launch();
       FM_TRY(check_launch("signal_tc_kernel"));
     }

@@ -27,17 +27,21 @@ def require_cuda() -> torch.device:
     return torch.device("cuda", torch.cuda.current_device())
 
 
+def _index(device: torch.device) -> int:
+    return device.index if device.index is not None else torch.cuda.current_device()
+
+
 def ctx_for(device: torch.device) -> int:
     """Library context of `device` bound to torch's current stream there."""
     stream = torch.cuda.current_stream(device)
-    return L.bind_stream(device.index, stream.cuda_stream)
+    return L.bind_stream(_index(device), stream.cuda_stream)
 
 
 def workspace(device: torch.device, nbytes: int) -> torch.Tensor:
     """A scratch buffer of at least nbytes, cached per (device, stream).  Work
     on one stream is ordered, so reusing the buffer there is safe."""
     stream = torch.cuda.current_stream(device)
-    key = (device.index, stream.cuda_stream)
+    key = (_index(device), stream.cuda_stream)
     buf = _ws_cache.get(key)
     if buf is None or buf.numel() < nbytes:
         buf = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8, device=device)

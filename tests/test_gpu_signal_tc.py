@@ -104,3 +104,23 @@ def test_deterministic_and_edge_cases(cuda):
         d = np.float64
         Signal(0, M, [p.astype(d) for p in traj.points], traj.t.astype(d), mesh.nodes, phi.astype(d), T2.astype(d),
                Mxy.astype(np.complex128), None, precision="bf16x3")
+
+
+def test_deep_node_sums_stay_accurate(cuda):
+    """Tens of thousands of nodes per sample: the tensor core's truncating FP32
+    accumulation must not grow with the node count (accumulators are drained
+    into round-to-nearest sums every 512 nodes)."""
+    mesh = W.tube(60_000, 0.012, 0.1)
+    N = mesh.n_nodes
+    rng = np.random.default_rng(5)
+    Mxy = ((rng.normal(size=(N, 4)) + 1j * rng.normal(size=(N, 4))) * 0.2).astype(np.complex64)
+    M = sp.diags(np.full(N, 2.3e-10)).tocsc()
+    phi = W.off_resonance(N)
+    _, T2 = W.tissue(N)
+    traj = W.cartesian(res=(4, 96, 32), fov=(0.1, 0.1, 0.1))
+    r0 = mesh.nodes.astype(np.float32)
+    K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    idx = np.random.default_rng(0).choice(traj.n_samples, 400, replace=False)
+    ref = _ref(M, traj, r0, phi, T2, Mxy, idx=idx)
+    err = fp64.rel_l2(K.reshape(-1, 4)[idx], ref)
+    assert err < 3e-5, err
