@@ -312,3 +312,4 @@ int fm_bloch_solve_f32(fm_ctx *ctx, const fm_bloch_args *a, void *workspace, siz
 }
 
 }  // extern "C"
+

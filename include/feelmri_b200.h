@@ -185,6 +185,7 @@ FM_API int fm_bloch_solve_f32(fm_ctx *ctx, const fm_bloch_args *args, void *work
                        size_t workspace_bytes);
 FM_API int fm_bloch_workspace_size(const fm_bloch_args *args, size_t *bytes);
 
+
 /* ---- MRI.Signal -------------------------------------------------------- */
 #define FM_PREC_F32 0        /* plain FP32 CUDA-core form (drop-in)            */
 #define FM_PREC_F64 1        /* FP64 form (the reference's double overload)    */

@@ -110,7 +110,11 @@ def test_motion_golden_host_classes_match_reference(cuda):
         gold = d[f"{name}/out"]
         for i, t in enumerate(d[f"{name}/t"]):
             y = np.broadcast_to(np.asarray(obj(float(t))), gold[i].shape)
-            np.testing.assert_allclose(y, gold[i], rtol=2e-6, atol=1e-9, equal_nan=True, err_msg=f"{name} t={t}")
+            # the modes x weights GEMV may sum in another order: float32 rounding
+            # of the largest terms bounds the difference
+            scale = np.nanmax(np.abs(gold)) if np.isfinite(gold).any() else 1.0
+            np.testing.assert_allclose(y, gold[i], rtol=1e-5, atol=2e-7 * scale, equal_nan=True,
+                                       err_msg=f"{name} t={t}")
 
 
 def test_motion_golden_device_weights_bit_exact(cuda):
@@ -155,4 +159,5 @@ def test_motion_golden_device_displacements(cuda):
         low = lower(obj, gold.shape[1], dev)
         assert low is not None, name
         disp = ops.motion_eval(low, gold.shape[1], d[f"{name}/t"], dev).cpu().numpy()
-        np.testing.assert_allclose(disp, gold, rtol=2e-6, atol=1e-9, equal_nan=True, err_msg=name)
+        scale = np.nanmax(np.abs(gold)) if np.isfinite(gold).any() else 1.0
+        np.testing.assert_allclose(disp, gold, rtol=1e-5, atol=2e-7 * scale, equal_nan=True, err_msg=name)
