@@ -155,6 +155,7 @@ SIGNATURES = {
     "fm_motion_eval_workspace_size": (C.c_int, [C.POINTER(Motion), _i64, _i64, C.POINTER(C.c_size_t)]),
     "fm_bloch_solve_f32": (C.c_int, [_p, C.POINTER(BlochArgs), _p, C.c_size_t]),
     "fm_bloch_workspace_size": (C.c_int, [C.POINTER(BlochArgs), C.POINTER(C.c_size_t)]),
+    "fm_bloch_solve_f32_noalloc": (C.c_int, [_p, C.POINTER(BlochArgs)]),
     "fm_signal": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, _p, C.c_size_t]),
     "fm_signal_workspace_size": (C.c_int, [C.POINTER(SignalArgs), C.c_int, C.POINTER(C.c_size_t)]),
     "fm_signal_count_time_runs": (C.c_int64, [_p, _i64, C.c_int]),

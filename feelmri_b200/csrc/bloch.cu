@@ -6,6 +6,8 @@
 // all time steps; per-step scalars (rf, G, dt, motion weights) are read as
 // warp-uniform loads.  Step i -> i+1 uses rf[i+1], G[i+1], dt[i+1]; dt[0] is
 // ignored; e1/e2 are recomputed only when dt changes (BlochSimulator.cpp:69-99).
+#include <mutex>
+
 #include "motion.cuh"
 
 namespace fm {
@@ -313,3 +315,49 @@ int fm_bloch_solve_f32(fm_ctx *ctx, const fm_bloch_args *a, void *workspace, siz
 
 }  // extern "C"
 
+// ---- no-allocation variant ---------------------------------------------
+// The per-step scratch of the sweep (step parameters, dt flags, motion call
+// times and weights) lives in this fixed array instead of a caller-provided
+// workspace.  Host code must not use the array's name as a device address:
+// its address is looked up once per device with cudaGetSymbolAddress.
+namespace fm {
+
+static __device__ __align__(256) unsigned char g_bloch_noalloc_scratch[FM_NOALLOC_BLOCH_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mutex;
+static void *g_noalloc_addr[128];
+
+// Device address of the scratch array on `device` (the current device).
+static int noalloc_scratch(int device, void **out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  FM_REQUIRE(device >= 0 && device < 128, FM_ERR_ARG, "fm_bloch_solve_f32_noalloc: device %d out of range", device);
+  if (g_noalloc_addr[device] == nullptr) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_bloch_noalloc_scratch);
+    FM_REQUIRE(e == cudaSuccess && ptr != nullptr, FM_ERR_CUDA,
+               "fm_bloch_solve_f32_noalloc: cudaGetSymbolAddress failed on device %d: %s", device,
+               cudaGetErrorString(e));
+    g_noalloc_addr[device] = ptr;
+  }
+  *out = g_noalloc_addr[device];
+  return FM_OK;
+}
+
+}  // namespace fm
+
+extern "C" int fm_bloch_solve_f32_noalloc(fm_ctx *ctx, const fm_bloch_args *a) {
+  using namespace fm;
+  FM_TRY(ctx_ok(ctx));
+  FM_TRY(validate_bloch(a));
+  DeviceGuard g(ctx->device);
+  FM_REQUIRE(g.ok, FM_ERR_CUDA, "fm_bloch_solve_f32_noalloc: cannot select device %d", ctx->device);
+  size_t need = 0;
+  FM_TRY(fm_bloch_workspace_size(a, &need));
+  FM_REQUIRE(need <= FM_NOALLOC_BLOCH_SCRATCH_BYTES, FM_ERR_NOMEM,
+             "fm_bloch_solve_f32_noalloc: %lld time steps need %zu bytes of scratch, more than the %u bytes this "
+             "entry point holds; use fm_bloch_solve_f32 with a workspace",
+             (long long)a->n_time, need, (unsigned)FM_NOALLOC_BLOCH_SCRATCH_BYTES);
+  void *scratch = nullptr;
+  FM_TRY(noalloc_scratch(ctx->device, &scratch));
+  return fm_bloch_solve_f32(ctx, a, scratch, FM_NOALLOC_BLOCH_SCRATCH_BYTES);
+}

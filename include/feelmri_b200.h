@@ -185,6 +185,27 @@ FM_API int fm_bloch_solve_f32(fm_ctx *ctx, const fm_bloch_args *args, void *work
                        size_t workspace_bytes);
 FM_API int fm_bloch_workspace_size(const fm_bloch_args *args, size_t *bytes);
 
+/* Scratch held by the library for fm_bloch_solve_f32_noalloc, per device. */
+#define FM_NOALLOC_BLOCH_SCRATCH_BYTES (4u << 20)
+
+/* Same computation as fm_bloch_solve_f32, for callers that cannot allocate
+ * device memory: code running where allocation is forbidden (inside a
+ * region another runtime is capturing, a real-time loop, or a host
+ * framework that owns every allocation through its own pool and offers no
+ * way to hand out a workspace).  The caller still provides every input and
+ * output buffer; the per-step scratch lives in a fixed-size array of device
+ * memory inside this library (FM_NOALLOC_BLOCH_SCRATCH_BYTES, enough for
+ * about 50,000 time steps with a 10-mode motion; larger requests are rejected
+ * with FM_ERR_NOMEM and the size they would need).  Every GPU that loads the
+ * library keeps that array until the process exits.
+ * The first call on a device looks up the array's device address (with that
+ * device current); make that first call before any stream capture.  All calls
+ * on a device share the one array, which keeps the previous call's contents
+ * (nothing in it needs to start at zero: each call writes every entry it
+ * reads), so calls that may overlap on the GPU -- on different streams or
+ * from different threads -- race and must be serialised by the caller.
+ * No counterpart in the reference: its solve_mri runs on the CPU. */
+FM_API int fm_bloch_solve_f32_noalloc(fm_ctx *ctx, const fm_bloch_args *args);
 
 /* ---- MRI.Signal -------------------------------------------------------- */
 #define FM_PREC_F32 0        /* plain FP32 CUDA-core form (drop-in)            */
