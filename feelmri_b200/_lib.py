@@ -151,12 +151,15 @@ SIGNATURES = {
     "fm_ctx_timing_query": (C.c_int, [_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "fm_pod_tensordot_f32": (C.c_int, [_p, _p, _p, _i64, _i64, _i64, _p]),
     "fm_pod_tensordot_f64": (C.c_int, [_p, _p, _p, _i64, _i64, _i64, _p]),
+    "fm_coil_expand": (C.c_int, [_p, _p, _p, _i64, _i64, _p]),
     "fm_motion_eval": (C.c_int, [_p, C.POINTER(Motion), _i64, _p, _i64, _p, _p, C.c_size_t]),
     "fm_motion_eval_workspace_size": (C.c_int, [C.POINTER(Motion), _i64, _i64, C.POINTER(C.c_size_t)]),
     "fm_bloch_solve_f32": (C.c_int, [_p, C.POINTER(BlochArgs), _p, C.c_size_t]),
     "fm_bloch_workspace_size": (C.c_int, [C.POINTER(BlochArgs), C.POINTER(C.c_size_t)]),
     "fm_bloch_solve_f32_noalloc": (C.c_int, [_p, C.POINTER(BlochArgs)]),
     "fm_signal": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, _p, C.c_size_t]),
+    "fm_signal_enqueue": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, _p, C.c_size_t]),
+    "fm_signal_status": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, _p, C.c_size_t]),
     "fm_signal_workspace_size": (C.c_int, [C.POINTER(SignalArgs), C.c_int, C.POINTER(C.c_size_t)]),
     "fm_signal_count_time_runs": (C.c_int64, [_p, _i64, C.c_int]),
     "fm_mass_assemble": (C.c_int, [_p, C.POINTER(MassArgs), C.c_int, C.POINTER(_i64), _p, _p, _p, _i64, _p,

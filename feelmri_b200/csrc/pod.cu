@@ -191,3 +191,31 @@ int fm_motion_eval(fm_ctx *ctx, const fm_motion *motion, int64_t n_nodes, const 
 }
 
 }  // extern "C"
+
+// ---- coil columns ---------------------------------------------------------
+// out[n, c] = m[n] * sens[n, c]: the transverse magnetisation seen by each
+// receive coil, the columns of Signal's Mxy when coils are simulated.  New
+// component: the reference's Signal takes no coil sensitivities.
+namespace fm {
+__global__ void coil_expand_kernel(const float2 *__restrict__ m, const float2 *__restrict__ sens, int64_t N,
+                                   int64_t C, float2 *__restrict__ out) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= N * C) return;
+  const int64_t n = idx / C;
+  const float2 a = m[n], b = sens[idx];
+  out[idx] = make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+}  // namespace fm
+
+extern "C" int fm_coil_expand(fm_ctx *ctx, const float *m, const float *sens, int64_t N, int64_t C, float *out) {
+  using namespace fm;
+  FM_TRY(ctx_ok(ctx));
+  FM_REQUIRE(N >= 0 && C >= 0, FM_ERR_SHAPE, "fm_coil_expand: negative extent");
+  if (N * C == 0) return FM_OK;
+  FM_REQUIRE(m && sens && out, FM_ERR_ARG, "fm_coil_expand: null pointer");
+  DeviceGuard g(ctx->device);
+  coil_expand_kernel<<<(unsigned)ceil_div(N * C, 256), 256, 0, ctx->stream>>>(
+      reinterpret_cast<const float2 *>(m), reinterpret_cast<const float2 *>(sens), N, C, reinterpret_cast<float2 *>(out));
+  count_launch();
+  return check_launch("coil_expand_kernel");
+}

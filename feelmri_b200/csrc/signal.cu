@@ -9,6 +9,9 @@ template <typename T>
 size_t plain_workspace(const fm_signal_args *a);
 int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes);
 size_t tc_workspace(const fm_signal_args *a);
+template <typename T>
+int signal_plain_errors(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes);
+int signal_tc_errors(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes);
 
 int validate_signal(const fm_signal_args *a, const char *who) {
   FM_REQUIRE(a != nullptr, FM_ERR_ARG, "%s: null args", who);
@@ -55,19 +58,43 @@ int fm_signal_workspace_size(const fm_signal_args *a, int precision, size_t *byt
   return FM_ERR_ARG;
 }
 
-int fm_signal(fm_ctx *ctx, const fm_signal_args *a, int precision, void *ws, size_t ws_bytes) {
+int fm_signal_enqueue(fm_ctx *ctx, const fm_signal_args *a, int precision, void *ws, size_t ws_bytes) {
   FM_TRY(ctx_ok(ctx));
-  FM_TRY(validate_signal(a, "fm_signal"));
+  FM_TRY(validate_signal(a, "fm_signal_enqueue"));
   DeviceGuard g(ctx->device);
-  FM_REQUIRE(g.ok, FM_ERR_CUDA, "fm_signal: cannot select device %d", ctx->device);
+  FM_REQUIRE(g.ok, FM_ERR_CUDA, "fm_signal_enqueue: cannot select device %d", ctx->device);
   switch (precision) {
     case FM_PREC_F32: return signal_plain<float>(ctx, a, ws, ws_bytes);
     case FM_PREC_F64: return signal_plain<double>(ctx, a, ws, ws_bytes);
     case FM_PREC_BF16X3: return signal_tc(ctx, a, ws, ws_bytes);
     default: break;
   }
-  set_error(FM_ERR_ARG, "fm_signal: unknown precision %d", precision);
+  set_error(FM_ERR_ARG, "fm_signal_enqueue: unknown precision %d", precision);
   return FM_ERR_ARG;
+}
+
+int fm_signal_status(fm_ctx *ctx, const fm_signal_args *a, int precision, void *ws, size_t ws_bytes) {
+  FM_TRY(ctx_ok(ctx));
+  FM_TRY(validate_signal(a, "fm_signal_status"));
+  DeviceGuard g(ctx->device);
+  const int64_t S = a->n_ro * a->n_lines * a->n_kz;
+  if (S == 0 || a->n_vencs == 0 || a->n_nodes == 0) {
+    FM_CUDA(cudaStreamSynchronize(ctx->stream));
+    return FM_OK;
+  }
+  switch (precision) {
+    case FM_PREC_F32: return signal_plain_errors<float>(ctx, a, ws, ws_bytes);
+    case FM_PREC_F64: return signal_plain_errors<double>(ctx, a, ws, ws_bytes);
+    case FM_PREC_BF16X3: return signal_tc_errors(ctx, a, ws, ws_bytes);
+    default: break;
+  }
+  set_error(FM_ERR_ARG, "fm_signal_status: unknown precision %d", precision);
+  return FM_ERR_ARG;
+}
+
+int fm_signal(fm_ctx *ctx, const fm_signal_args *a, int precision, void *ws, size_t ws_bytes) {
+  FM_TRY(fm_signal_enqueue(ctx, a, precision, ws, ws_bytes));
+  return fm_signal_status(ctx, a, precision, ws, ws_bytes);
 }
 
 int64_t fm_signal_count_time_runs(const void *t_host, int64_t n_samples, int is_double) {

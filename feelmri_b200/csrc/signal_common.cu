@@ -24,7 +24,8 @@ void carve_runs(Carve &c, int64_t S, int tile, Runs &r) {
   r.tile_run = c.take<int>(mt);
   r.tile_s0 = c.take<int>(mt);
   r.run_t = c.take<double>(S + 1);
-  r.counts = c.take<int>(4);
+  r.counts = c.take<int>(8);
+  r.error = c.take<int>(4);
   r.cub_bytes = cub_scan_bytes(S + 1);
   r.cub_tmp = c.take<char>(r.cub_bytes);
 }
@@ -67,11 +68,11 @@ __global__ void run_starts_kernel(const T *__restrict__ t, int64_t S, const int 
 }
 
 __global__ void run_ntiles_kernel(const int *__restrict__ start, const int *__restrict__ counts, int tile,
-                                  int *__restrict__ ntiles) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+                                  int *__restrict__ ntiles, int64_t S) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = counts[0];
-  if (g > n) return;
-  ntiles[g] = (g == n) ? 0 : (start[g + 1] - start[g] + tile - 1) / tile;
+  if (g > S) return;
+  ntiles[g] = (g >= n) ? 0 : (start[g + 1] - start[g] + tile - 1) / tile;
 }
 
 __global__ void run_tiles_kernel(const int *__restrict__ start, const int *__restrict__ tile_off,
@@ -91,8 +92,9 @@ __global__ void run_tiles_kernel(const int *__restrict__ start, const int *__res
 }
 
 template <typename T>
-int build_runs(const T *t, int64_t S, int tile, Runs &r, cudaStream_t st, int *n_runs, int *n_tiles) {
+int build_runs(const T *t, int64_t S, int tile, Runs &r, cudaStream_t st) {
   const unsigned b = (unsigned)ceil_div(S, 256);
+  FM_CUDA(cudaMemsetAsync(r.error, 0, sizeof(int), st));
   run_flags_kernel<T><<<b, 256, 0, st>>>(t, S, r.flag);
   count_launch();
   FM_TRY(check_launch("run_flags_kernel"));
@@ -104,7 +106,7 @@ int build_runs(const T *t, int64_t S, int tile, Runs &r, cudaStream_t st, int *n
   FM_TRY(check_launch("run_starts_kernel"));
   // tile counts per run, then exclusive scan over n_runs + 1 entries (the
   // scan length is bounded by S + 1; unused tail entries are zero).
-  run_ntiles_kernel<<<(unsigned)ceil_div(S + 1, 256), 256, 0, st>>>(r.start, r.counts, tile, r.flag);
+  run_ntiles_kernel<<<(unsigned)ceil_div(S + 1, 256), 256, 0, st>>>(r.start, r.counts, tile, r.flag, S);
   count_launch();
   FM_TRY(check_launch("run_ntiles_kernel"));
   cb = r.cub_bytes;
@@ -113,17 +115,63 @@ int build_runs(const T *t, int64_t S, int tile, Runs &r, cudaStream_t st, int *n
   run_tiles_kernel<<<(unsigned)ceil_div(S + 1, 256), 256, 0, st>>>(r.start, r.tile_off, r.counts, tile, r.tile_run,
                                                                    r.tile_s0);
   count_launch();
-  FM_TRY(check_launch("run_tiles_kernel"));
-  int h[2] = {0, 0};
-  FM_CUDA(cudaMemcpyAsync(h, r.counts, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  return check_launch("run_tiles_kernel");
+}
+
+__global__ void table_calls_kernel(const int *__restrict__ counts, int64_t calls, int *__restrict__ error) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && counts[0] != calls) atomicOr(error, kErrTableCalls);
+}
+
+int check_table_calls(const fm_motion *m, Runs &r, cudaStream_t st) {
+  if (m == nullptr || m->kind != FM_MOTION_TABLE) return FM_OK;
+  table_calls_kernel<<<1, 32, 0, st>>>(r.counts, m->table_calls, r.error);
+  count_launch();
+  return check_launch("table_calls_kernel");
+}
+
+int report_errors(Runs &r, cudaStream_t st, const char *who) {
+  int h = 0;
+  FM_CUDA(cudaMemcpyAsync(&h, r.error, sizeof(int), cudaMemcpyDeviceToHost, st));
   FM_CUDA(cudaStreamSynchronize(st));
-  *n_runs = h[0];
-  *n_tiles = h[1];
+  FM_REQUIRE(!(h & kErrSparseRow), FM_ERR_SHAPE, "%s: sparse M has a row index outside [0, rows)", who);
+  FM_REQUIRE(!(h & kErrTableCalls), FM_ERR_SHAPE,
+             "%s: TABLE motion must hold one entry per distinct-time run of t", who);
+  FM_REQUIRE(!(h & kErrTimeout), FM_ERR_TIMEOUT, "%s: a tensor-core pipeline wait timed out", who);
   return FM_OK;
 }
 
-template int build_runs<float>(const float *, int64_t, int, Runs &, cudaStream_t, int *, int *);
-template int build_runs<double>(const double *, int64_t, int, Runs &, cudaStream_t, int *, int *);
+__global__ void run_weights_kernel(MotionDev md, const double *__restrict__ times, const int *__restrict__ n_runs,
+                                   float *__restrict__ weights) {
+  const int64_t total = (int64_t)n_runs[0] * md.slots;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = idx / md.slots;
+    const int s = (int)(idx - c * md.slots);
+    int k = 0;
+    while (k + 1 < md.n_terms && s >= md.slot0[k + 1]) ++k;
+    const fm_motion_term &T = md.terms[k];
+    const double t = times[c];
+    const double v = ppoly_eval(T.pp_c, T.pp_x, T.pp_k, T.pp_intervals, T.n_modes, s - md.slot0[k],
+                                term_time(t, T), T.extrapolate);
+    float w = __double2float_rn(v);
+    if (T.kind == FM_TERM_POD_VELOCITY) w = __fmul_rn(w, __double2float_rn(t));
+    weights[idx] = w;
+  }
+}
+
+int launch_run_weights(const MotionDev &md, const double *run_t, const int *n_runs, int64_t max_runs,
+                       float *weights, cudaStream_t st) {
+  if (md.kind != FM_MOTION_TERMS || max_runs == 0) return FM_OK;
+  const int64_t total = max_runs * md.slots;
+  int64_t blocks = ceil_div(total, 256);
+  if (blocks > 4 * kSmCount) blocks = 4 * kSmCount;
+  run_weights_kernel<<<(unsigned)blocks, 256, 0, st>>>(md, run_t, n_runs, weights);
+  count_launch();
+  return check_launch("run_weights_kernel");
+}
+
+template int build_runs<float>(const float *, int64_t, int, Runs &, cudaStream_t);
+template int build_runs<double>(const double *, int64_t, int, Runs &, cudaStream_t);
 
 // ---- CSC -> CSR in Eigen's accumulation order ---------------------------
 
@@ -133,7 +181,7 @@ __global__ void csr_count_kernel(const int *__restrict__ indices, int64_t nnz, i
   if (k >= nnz) return;
   const int i = indices[k];
   if (i < 0 || i >= rows) {
-    atomicExch(bad, 1);
+    atomicOr(bad, kErrSparseRow);
     return;
   }
   atomicAdd(cnt + i, 1);
@@ -203,22 +251,17 @@ __global__ void spmm_kernel(const int *__restrict__ rowptr, const int *__restric
 }
 
 template <typename T>
-int sparse_times_dense(const fm_signal_args *a, Csr &m, const T *Mxy, T *MM, cudaStream_t st) {
+int sparse_times_dense(const fm_signal_args *a, Csr &m, const T *Mxy, T *MM, int *error, cudaStream_t st) {
   const int64_t rows = a->m_rows, cols = a->m_cols, nnz = a->m_nnz, V = a->n_vencs;
   FM_CUDA(cudaMemsetAsync(m.fill, 0, (rows + 1) * sizeof(int), st));
-  int *bad = m.fill + rows;  // last slot doubles as the out-of-range flag
   if (nnz > 0) {
-    csr_count_kernel<<<(unsigned)ceil_div(nnz, 256), 256, 0, st>>>(a->m_indices, nnz, rows, m.fill, bad);
+    csr_count_kernel<<<(unsigned)ceil_div(nnz, 256), 256, 0, st>>>(a->m_indices, nnz, rows, m.fill, error);
     count_launch();
     FM_TRY(check_launch("csr_count_kernel"));
   }
   size_t cb = m.cub_bytes;
   FM_CUDA(cub::DeviceScan::ExclusiveSum(m.cub_tmp, cb, m.fill, m.rowptr, (int)(rows + 1), st));
   count_launch();
-  int hbad = 0;
-  FM_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
-  FM_CUDA(cudaStreamSynchronize(st));
-  FM_REQUIRE(hbad == 0, FM_ERR_SHAPE, "fm_signal: sparse M has a row index outside [0, %lld)", (long long)rows);
   FM_CUDA(cudaMemsetAsync(m.fill, 0, (rows + 1) * sizeof(int), st));
   if (cols > 0 && nnz > 0) {
     csr_scatter_kernel<<<(unsigned)ceil_div(cols, 256), 256, 0, st>>>(a->m_indptr, a->m_indices, cols, rows,
@@ -240,7 +283,8 @@ int sparse_times_dense(const fm_signal_args *a, Csr &m, const T *Mxy, T *MM, cud
   return FM_OK;
 }
 
-template int sparse_times_dense<float>(const fm_signal_args *, Csr &, const float *, float *, cudaStream_t);
-template int sparse_times_dense<double>(const fm_signal_args *, Csr &, const double *, double *, cudaStream_t);
+template int sparse_times_dense<float>(const fm_signal_args *, Csr &, const float *, float *, int *, cudaStream_t);
+template int sparse_times_dense<double>(const fm_signal_args *, Csr &, const double *, double *, int *,
+                                        cudaStream_t);
 
 }  // namespace fm

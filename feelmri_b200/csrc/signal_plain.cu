@@ -35,6 +35,7 @@ struct PlainDev {
   const float *weights;   // (n_runs, slots) TERMS motion weights
   const T *table;         // TABLE motion (n_runs, N, 3) in T
   const int *tile_run, *tile_s0, *run_start;
+  const int *n_tiles;     // device: number of tiles
   const double *run_t;
   int64_t chunk;          // nodes per split
   int splits;
@@ -62,8 +63,10 @@ __global__ void __launch_bounds__(kPlainThreads) signal_plain_kernel(PlainDev<T>
   __shared__ T4 s_pos[NT];             // moved x, y, z and phi * t
   __shared__ T s_w[NT][2 * VMAX];      // decayed M * Mxy columns v0 .. v0 + VMAX
 
-  const int tile = blockIdx.x;
+  const int n_tiles = *p.n_tiles;
   const int split = blockIdx.y;
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  __syncthreads();  // the previous tile's readers of s_pos / s_w are done
   const int g = p.tile_run[tile];
   const int s_begin = p.tile_s0[tile];
   const int s_end = min(p.run_start[g + 1], s_begin + kPlainThreads * SPT);
@@ -149,6 +152,7 @@ __global__ void __launch_bounds__(kPlainThreads) signal_plain_kernel(PlainDev<T>
       }
     }
   }
+  }  // tiles
 }
 
 // out[e] = sum over splits in order of partial[split][e].
@@ -162,9 +166,10 @@ __global__ void split_reduce_kernel(const T *__restrict__ part, int splits, int6
 }
 
 template <typename T, int VMAX>
-static void launch_plain(const PlainDev<T> &p, int n_tiles, int v0, int spt, cudaStream_t st) {
+static void launch_plain(const PlainDev<T> &p, int64_t max_tiles, int v0, int spt, cudaStream_t st) {
   constexpr int NT = 128;
-  dim3 grid((unsigned)n_tiles, (unsigned)p.splits);
+  const int64_t per_split = (4LL * kSmCount + p.splits - 1) / p.splits;
+  dim3 grid((unsigned)(max_tiles < per_split ? max_tiles : per_split), (unsigned)p.splits);
   if (spt == 2) signal_plain_kernel<T, VMAX, 2, NT><<<grid, kPlainThreads, 0, st>>>(p, v0);
   else signal_plain_kernel<T, VMAX, 1, NT><<<grid, kPlainThreads, 0, st>>>(p, v0);
 }
@@ -228,16 +233,12 @@ int signal_plain(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes
     FM_CUDA(cudaMemsetAsync(out, 0, (size_t)S * V * 2 * sizeof(T), st));
     return FM_OK;
   }
-  FM_TRY(sparse_times_dense<T>(a, pl.csr, static_cast<const T *>(a->Mxy), pl.MM, st));
-  int n_runs = 0, n_tiles = 0;
-  FM_TRY(build_runs<T>(static_cast<const T *>(a->t), S, pl.tile, pl.runs, st, &n_runs, &n_tiles));
+  FM_TRY(build_runs<T>(static_cast<const T *>(a->t), S, pl.tile, pl.runs, st));
+  FM_TRY(sparse_times_dense<T>(a, pl.csr, static_cast<const T *>(a->Mxy), pl.MM, pl.runs.error, st));
+  FM_TRY(check_table_calls(a->motion, pl.runs, st));
   const MotionDev md = make_motion_dev(a->motion);
-  if (a->motion && a->motion->kind == FM_MOTION_TABLE) {
-    FM_REQUIRE(a->motion->table_calls == n_runs, FM_ERR_SHAPE,
-               "%s: TABLE motion holds %lld entries but t has %d distinct-time runs", who,
-               (long long)a->motion->table_calls, n_runs);
-  }
-  FM_TRY(launch_motion_weights(md, pl.runs.run_t, n_runs, pl.weights, st));
+  FM_TRY(launch_run_weights(md, pl.runs.run_t, pl.runs.counts, S, pl.weights, st));
+  const int64_t max_tiles = max_tiles_for(S, pl.tile);
 
   PlainDev<T> p{};
   p.N = N; p.S = S; p.V = V;
@@ -251,6 +252,7 @@ int signal_plain(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes
   p.md = md;
   p.weights = (md.kind == FM_MOTION_TERMS) ? pl.weights : nullptr;
   p.table = (a->motion && a->motion->kind == FM_MOTION_TABLE) ? static_cast<const T *>(a->motion->table) : nullptr;
+  p.n_tiles = pl.runs.counts + 1;
   p.tile_run = pl.runs.tile_run;
   p.tile_s0 = pl.runs.tile_s0;
   p.run_start = pl.runs.start;
@@ -266,10 +268,10 @@ int signal_plain(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes
   ScopedTimer timer(ctx, sizeof(T) == 4 ? "signal_f32" : "signal_f64");
   for (int v0 = 0; v0 < V; v0 += 8) {
     const int64_t nv = V - v0;
-    if (nv <= 1) launch_plain<T, 1>(p, n_tiles, v0, spt, st);
-    else if (nv <= 2) launch_plain<T, 2>(p, n_tiles, v0, spt, st);
-    else if (nv <= 4) launch_plain<T, 4>(p, n_tiles, v0, spt, st);
-    else launch_plain<T, 8>(p, n_tiles, v0, spt, st);
+    if (nv <= 1) launch_plain<T, 1>(p, max_tiles, v0, spt, st);
+    else if (nv <= 2) launch_plain<T, 2>(p, max_tiles, v0, spt, st);
+    else if (nv <= 4) launch_plain<T, 4>(p, max_tiles, v0, spt, st);
+    else launch_plain<T, 8>(p, max_tiles, v0, spt, st);
     count_launch();
     FM_TRY(check_launch("signal_plain_kernel"));
   }
@@ -281,6 +283,17 @@ int signal_plain(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes
   }
   return FM_OK;
 }
+
+template <typename T>
+int signal_plain_errors(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
+  Carve cv(ws, ws_bytes);
+  PlainPlan<T> pl;
+  carve_plain<T>(cv, a, pl);
+  FM_TRY(carve_ok(cv, "fm_signal"));
+  return report_errors(pl.runs, ctx->stream, sizeof(T) == 4 ? "fm_signal(F32)" : "fm_signal(F64)");
+}
+template int signal_plain_errors<float>(fm_ctx *, const fm_signal_args *, void *, size_t);
+template int signal_plain_errors<double>(fm_ctx *, const fm_signal_args *, void *, size_t);
 
 template int signal_plain<float>(fm_ctx *, const fm_signal_args *, void *, size_t);
 template int signal_plain<double>(fm_ctx *, const fm_signal_args *, void *, size_t);

@@ -46,7 +46,7 @@ constexpr int kTcBlockNodes = 128;  // nodes whose per-run data is formed togeth
 constexpr int kTcProducers = 256;   // warps 0-7
 constexpr int kTcMmaWarp = 8;
 constexpr int kTcThreads = 288;
-constexpr int kTcVGroup = 16;       // Mxy columns per launch
+constexpr int kTcVGroup = 8;        // Mxy columns per launch
 // Stages accumulated in one tensor-memory accumulator before it is drained
 // into an FP32 round-to-nearest running sum.  The tensor core's FP32
 // accumulation truncates, so its error grows with the number of MMAs added
@@ -79,6 +79,8 @@ struct TcDev {
   int Qt, NT, acc_cols;
   int splits;
   int64_t chunk;
+  const int *plan;  // device: [2] factored items, [3] generic items, [4] splits, [5] nodes per split
+  float2 *partials; // (splits, S, V) when splits > 1
   float2 *out;
   float *scratch;  // per block: 128 x NT running sums
   int *error;
@@ -86,9 +88,10 @@ struct TcDev {
 
 struct TcSmem {
   uint32_t stage_bytes, a_hi, a_lo, b_hi, b_lo;  // offsets inside a stage
-  uint32_t pos, w, etab, kq, bars, misc, total;
+  uint32_t posd, valid, w, etab, kq, bars, misc, total;
 };
 
+// Node data is double-buffered: block b is read while block b + 1 is written.
 __host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
   TcSmem L;
   L.a_hi = 0;
@@ -97,17 +100,19 @@ __host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
   L.b_lo = 2 * kAStageBytes + NT * 2 * kTcNodes * 2;
   L.stage_bytes = 2 * kAStageBytes + 2 * NT * 2 * kTcNodes * 2;
   uint32_t off = kTcStages * L.stage_bytes;
-  L.pos = off;
-  off += kTcBlockNodes * 16;
-  L.w = off;
-  off += kTcBlockNodes * VG * 8;
-  L.etab = off;
-  off += Qt * kTcNodes * 8;
-  L.kq = off;
+  L.posd = off;  // [2][128] double4 (x, y, z, unused)
+  off += 2 * kTcBlockNodes * 32;
+  L.valid = off;  // [2][128] float
+  off += 2 * kTcBlockNodes * 4;
+  L.w = off;  // [2][128][VG] float2
+  off += 2 * kTcBlockNodes * VG * 8;
+  L.etab = off;  // [2][Qt][16] float2, by stage parity
+  off += 2 * Qt * kTcNodes * 8;
+  L.kq = off;  // [Qt][3] double
   off += ((Qt * 24 + 15) / 16) * 16;
   L.bars = off;
   off += 16 * 8;
-  L.misc = off;
+  L.misc = off;  // tmem address, abort flag
   off += 16;
   L.total = off;
   return L;
@@ -121,51 +126,26 @@ __device__ inline uint32_t kmajor_offset(uint32_t row, uint32_t k, uint32_t rows
   return (k >> 4) * (rows * 32) + (row >> 3) * 256 + ((k >> 3) & 1) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
-__device__ inline uint32_t pack_bf16(float a, float b) {
-  __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-  return *reinterpret_cast<uint32_t *>(&h);
+__device__ inline uint32_t bf16x2_bits(__nv_bfloat162 h) { return *reinterpret_cast<uint32_t *>(&h); }
+
+// hi = bf16(x), lo = bf16(x - hi) for the pair (a, b); bits of (hi_a, hi_b)
+// and (lo_a, lo_b) with a in the low half.
+__device__ inline void split_pair(float a, float b, uint32_t &hi, uint32_t &lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  const float2 hf = __bfloat1622float2(h);
+  hi = bf16x2_bits(h);
+  lo = bf16x2_bits(__floats2bfloat162_rn(a - hf.x, b - hf.y));
 }
 
-// hi/lo split of 8 consecutive K values written as one 16-byte chunk each.
-__device__ inline void store_split8(uint32_t hi_addr, uint32_t lo_addr, const float (&x)[8]) {
-  uint32_t h[4], l[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    __nv_bfloat162 hb = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
-    const float2 hf = __bfloat1622float2(hb);
-    h[i] = *reinterpret_cast<uint32_t *>(&hb);
-    l[i] = pack_bf16(x[2 * i] - hf.x, x[2 * i + 1] - hf.y);
-  }
-  ptx::st_shared_v4(hi_addr, h[0], h[1], h[2], h[3]);
-  ptx::st_shared_v4(lo_addr, l[0], l[1], l[2], l[3]);
-}
-
-__device__ inline void store_zero8(uint32_t hi_addr, uint32_t lo_addr) {
-  ptx::st_shared_v4(hi_addr, 0u, 0u, 0u, 0u);
-  ptx::st_shared_v4(lo_addr, 0u, 0u, 0u, 0u);
-}
-
-// exp(-2 pi i c) for c in cycles given in FP64: reduce modulo one, then FP32.
+// exp(-2 pi i c) for c in cycles given in FP64: reduce modulo one with an
+// exact round-to-integer (add/subtract 1.5 * 2^52), then FP32 sin/cos.
 __device__ inline float2 cis_neg_cycles(double c) {
-  const double f = c - rint(c);
+  const double kRound = 6755399441055744.0;
+  const double n = __dsub_rn(__dadd_rn(c, kRound), kRound);
+  const float f = __double2float_rn(__dsub_rn(c, n));
   float s, co;
-  __sincosf(6.283185307179586f * (float)f, &s, &co);
+  __sincosf(6.283185307179586f * f, &s, &co);
   return make_float2(co, -s);
-}
-
-// OR of a predicate over the 256 producer threads (named barrier 1): used
-// for every decision that must be uniform across them.
-__device__ inline bool producers_any(bool x) {
-  uint32_t out;
-  asm volatile(
-      "{\n\t.reg .pred pi, po;\n\t"
-      "setp.ne.u32 pi, %1, 0;\n\t"
-      "bar.red.or.pred po, 1, 256, pi;\n\t"
-      "selp.u32 %0, 1, 0, po;\n\t}"
-      : "=r"(out)
-      : "r"((uint32_t)x)
-      : "memory");
-  return out != 0;
 }
 
 struct TcUnit {
@@ -190,16 +170,73 @@ __device__ inline TcUnit tc_unit(const TcDev &p, int u) {
   return U;
 }
 
-// Adds accumulator `buf` (one drained group) into the block's running sums,
+// Bounded wait that gives up at once after any earlier timeout of the block
+// (the flag lives in shared memory), so a broken pipeline ends quickly.
+__device__ inline bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
+  if (*abort_flag) return false;
+  if (ptx::mbar_wait(bar, parity, kTcWaitNs)) return true;
+  *abort_flag = 1;
+  return false;
+}
+
+// Raw node data loaded one node block ahead (global loads in flight while
+// the current block is processed).
+struct TcRaw {
+  float x, y, z, t2, phi;
+  float2 m[kTcVGroup];
+};
+
+__device__ inline void tc_load_raw(const TcDev &p, int64_t n, TcRaw &r) {
+  r.x = p.r0[3 * n + 0];
+  r.y = p.r0[3 * n + 1];
+  r.z = p.r0[3 * n + 2];
+  r.t2 = p.T2[n];
+  r.phi = p.phi[n];
+#pragma unroll
+  for (int v = 0; v < kTcVGroup; ++v)
+    if (v < p.VG) r.m[v] = p.MM[n * p.V + p.v0 + v];
+}
+
+// Per-run node quantities of one node into buffer `buf`: moved position (in
+// FP64 for the phase products), validity and the decayed, off-resonance
+// rotated weights W' = (M Mxy)[n, v] exp(-t / T2) exp(i phi t).
+__device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, const TcRaw &r, const float *wrun,
+                                 float tg, double4 *posd, float *valid, float2 *wblk, int slot) {
+  if (n < U.n_end) {
+    float x = r.x, y = r.y, z = r.z;
+    if (p.md.kind == FM_MOTION_TERMS) {
+      float dx, dy, dz;
+      motion_disp(p.md, wrun, n, p.N, dx, dy, dz);
+      x = x + dx; y = y + dy; z = z + dz;
+    } else if (p.table) {
+      const float *d = p.table + ((int64_t)U.it.run * p.N + n) * 3;
+      x = x + d[0]; y = y + d[1]; z = z + d[2];
+    }
+    posd[slot] = make_double4((double)x, (double)y, (double)z, 0.0);
+    valid[slot] = 1.f;
+    const float decay = expf(-tg * (1.0f / r.t2));
+    float so, co;
+    sincosf(r.phi * tg, &so, &co);
+    const float er = decay * co, ei = decay * so;
+#pragma unroll
+    for (int v = 0; v < kTcVGroup; ++v)
+      if (v < p.VG) wblk[slot * p.VG + v] = make_float2(r.m[v].x * er - r.m[v].y * ei, r.m[v].x * ei + r.m[v].y * er);
+  } else {
+    posd[slot] = make_double4(0.0, 0.0, 0.0, 0.0);
+    valid[slot] = 0.f;
+    for (int v = 0; v < p.VG; ++v) wblk[slot * p.VG + v] = make_float2(0.f, 0.f);
+  }
+}
+
+// Adds accumulator `b` (one drained group) into the block's running sums,
 // or, for the unit's last group, writes running sums + accumulator to the
 // output samples.  Executed by all 256 producers: warp w reads TMEM lanes of
 // quarter w % 4 and column half w / 4.
-__device__ inline bool tc_drain(const TcDev &p, const TcUnit &U, uint64_t *accfull, uint64_t *accfree, uint32_t tmem,
-                                int gg, bool first, bool final, bool ok_in) {
+__device__ inline void tc_drain(const TcDev &p, const TcUnit &U, uint64_t *accfull, uint64_t *accfree, uint32_t tmem,
+                                int gg, bool first, bool final, volatile int *abort_flag) {
   const int tid = threadIdx.x, warp = tid >> 5;
   const int b = gg & 1;
-  const bool waited = ptx::mbar_wait(&accfull[b], (gg >> 1) & 1, kTcWaitNs);
-  const bool ok = ok_in && !producers_any(!waited);
+  tc_wait(&accfull[b], (gg >> 1) & 1, abort_flag);
   ptx::tc_fence_after();
   const int quarter = warp & 3, half = warp >> 2;
   const int row = quarter * 32 + (tid & 31);
@@ -211,13 +248,8 @@ __device__ inline bool tc_drain(const TcDev &p, const TcUnit &U, uint64_t *accfu
   const int s_row = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz + U.it.q0 : U.it.p0 + row);
   for (int c0 = c_begin; c0 < c_end; c0 += 16) {
     uint32_t r[16];
-    if (ok) {
-      ptx::tmem_ld16(tmem + (uint32_t)(b * p.acc_cols) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, r);
-      ptx::tmem_wait_ld();
-    } else {
-#pragma unroll
-      for (int i = 0; i < 16; ++i) r[i] = 0u;
-    }
+    ptx::tmem_ld16(tmem + (uint32_t)(b * p.acc_cols) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, r);
+    ptx::tmem_wait_ld();
     if (!row_ok) continue;
     float v[16];
 #pragma unroll
@@ -245,11 +277,19 @@ __device__ inline bool tc_drain(const TcDev &p, const TcUnit &U, uint64_t *accfu
   }
   ptx::tc_fence_before();
   ptx::mbar_arrive(&accfree[b]);
-  return ok;
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n_units) {
+__global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p_in, int kind) {
   extern __shared__ __align__(1024) unsigned char smem[];
+  // work sizes come from the device-side plan, so the launch needs no host
+  // synchronisation (and can be captured in a CUDA graph)
+  TcDev p = p_in;
+  p.splits = p_in.plan[4];
+  p.chunk = p_in.plan[5];
+  p.item0 = kind == 0 ? 0 : p_in.plan[2];
+  p.n_items = kind == 0 ? p_in.plan[2] : p_in.plan[3];
+  p.out = p.splits > 1 ? p_in.partials : p_in.out;
+  const int n_units = p.n_items * p.splits;
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
   const TcSmem L = tc_smem_layout(p.NT, p.VG, p.Qt);
@@ -259,8 +299,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n
   uint64_t *accfree = accfull + 2;
   uint64_t *done = accfree + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L.misc);
-  float4 *pos = reinterpret_cast<float4 *>(smem + L.pos);
-  float2 *wblk = reinterpret_cast<float2 *>(smem + L.w);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + L.misc + 4);
+  double4 *posd_all = reinterpret_cast<double4 *>(smem + L.posd);
+  float *valid_all = reinterpret_cast<float *>(smem + L.valid);
+  float2 *w_all = reinterpret_cast<float2 *>(smem + L.w);
   float2 *etab = reinterpret_cast<float2 *>(smem + L.etab);
   double *kq = reinterpret_cast<double *>(smem + L.kq);
   const uint32_t sbase = ptx::smem_addr(smem);
@@ -275,6 +317,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n
       ptx::mbar_init(&accfree[b], kTcProducers);
     }
     ptx::mbar_init(done, 1);
+    *abort_flag = 0;
     ptx::fence_mbar_init();
   }
   if (warp == kTcMmaWarp) ptx::tmem_alloc(tmem_slot, 2 * p.acc_cols);
@@ -283,16 +326,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n
   ptx::tc_fence_after();
   const uint32_t tmem = tmem_slot[0];
   const uint32_t idesc = ptx::idesc_bf16_f32(kTcRows, p.NT);
-  bool ok = true;
 
   if (warp < kTcMmaWarp) {
     // ------------------------------------------------------ producers --
     const int row = tid & (kTcRows - 1);  // A row / B (q, v) pair of this thread
     const int half = tid >> 7;            // which 8 of the 16 nodes of a stage
+    const bool loader = tid < kTcBlockNodes;
     int gst = 0, gbase = 0;
-    for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
+    TcRaw raw;
+    for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
       const TcUnit U = tc_unit(p, u);
-      ptx::named_barrier(1, kTcProducers);  // previous unit's readers of kq are done
+      ptx::named_barrier(1, kTcProducers);  // the previous unit's readers are done
       for (int q = tid; q < U.Q_tile; q += kTcProducers) {
         const int s_q = U.run.start + U.it.q0 + q, s_0 = U.run.start;
         kq[3 * q + 0] = U.run.factored ? (double)p.kx[s_q] - (double)p.kx[s_0] : 0.0;
@@ -312,60 +356,54 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n
       const int bq = b_active ? row / p.VG : 0, bv = b_active ? row % p.VG : 0;
       const float *wrun = p.weights ? p.weights + (int64_t)U.it.run * p.md.slots : nullptr;
       const float tg = (float)p.run_t[U.it.run];
+      const int n_blocks = (int)ceil_div(U.n_stages, kTcBlockNodes / kTcNodes);
+      // prologue: node block 0 into buffer 0, block 1's loads in flight
+      if (loader && U.n_stages > 0) {
+        const int64_t n = U.n_begin + tid;
+        if (n < U.n_end) tc_load_raw(p, n, raw);
+        tc_derive(p, U, n, raw, wrun, tg, posd_all, valid_all, w_all, tid);
+        const int64_t n1 = n + kTcBlockNodes;
+        if (n_blocks > 1 && n1 < U.n_end) tc_load_raw(p, n1, raw);
+      }
       int next_drain = 0;
 
       for (int st = 0; st < U.n_stages; ++st, ++gst) {
         const int s = gst % kTcStages;
         const uint32_t round = gst / kTcStages;
         const int j = st % (kTcBlockNodes / kTcNodes);
+        const int blk = st / (kTcBlockNodes / kTcNodes);
+        const int buf = blk & 1;
         if (j == 0) {
+          // buffer `buf` (written during the previous block) is complete, and
+          // every producer is done with the other buffer
           ptx::named_barrier(1, kTcProducers);
-          if (tid < kTcBlockNodes) {
-            const int64_t n = U.n_begin + (int64_t)st * kTcNodes + tid;
-            float4 pp = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (n < U.n_end) {
-              float x = p.r0[3 * n + 0], y = p.r0[3 * n + 1], z = p.r0[3 * n + 2];
-              if (p.md.kind == FM_MOTION_TERMS) {
-                float dx, dy, dz;
-                motion_disp(p.md, wrun, n, p.N, dx, dy, dz);
-                x = x + dx; y = y + dy; z = z + dz;
-              } else if (p.table) {
-                const float *d = p.table + ((int64_t)U.it.run * p.N + n) * 3;
-                x = x + d[0]; y = y + d[1]; z = z + d[2];
-              }
-              pp = make_float4(x, y, z, 1.f);
-              const float decay = expf(-tg * (1.0f / p.T2[n]));
-              float so, co;
-              sincosf(p.phi[n] * tg, &so, &co);
-              const float er = decay * co, ei = decay * so;
-              for (int v = 0; v < p.VG; ++v) {
-                const float2 m = p.MM[n * p.V + p.v0 + v];
-                wblk[tid * p.VG + v] = make_float2(m.x * er - m.y * ei, m.x * ei + m.y * er);
-              }
-            } else {
-              for (int v = 0; v < p.VG; ++v) wblk[tid * p.VG + v] = make_float2(0.f, 0.f);
-            }
-            pos[tid] = pp;
+          if (loader && blk >= 1 && blk + 1 < n_blocks) {
+            const int64_t n2 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes + tid;
+            if (n2 < U.n_end) tc_load_raw(p, n2, raw);
           }
-          ptx::named_barrier(1, kTcProducers);
         }
+        if (j == 4 && loader && blk + 1 < n_blocks) {
+          const int64_t n1 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes + tid;
+          tc_derive(p, U, n1, raw, wrun, tg, posd_all + (buf ^ 1) * kTcBlockNodes,
+                    valid_all + (buf ^ 1) * kTcBlockNodes, w_all + (buf ^ 1) * kTcBlockNodes * p.VG, tid);
+        }
+        const double4 *pn = posd_all + buf * kTcBlockNodes + j * kTcNodes;
+        const float *vn = valid_all + buf * kTcBlockNodes + j * kTcNodes;
+        const float2 *wn = w_all + (buf * kTcBlockNodes + j * kTcNodes) * p.VG;
         // wait until the MMAs that last read stage s are done
-        const bool waited = ptx::mbar_wait(&empty[s], (round & 1) ^ 1, kTcWaitNs);
-        if (producers_any(!waited)) {
-          ok = false;
-          break;
-        }
-        const float4 *pn = pos + j * kTcNodes;
-        const float2 *wn = wblk + j * kTcNodes * p.VG;
+        tc_wait(&empty[s], (round & 1) ^ 1, abort_flag);
+        // e_q(n) = exp(-2 pi i kq_q . r_n) for this stage's nodes.  Buffers
+        // alternate by stage: a thread that writes stage st's table has passed
+        // the barrier of stage st - 1, so every reader of stage st - 2 is done.
+        float2 *et = etab + (st & 1) * p.Qt * kTcNodes;
         for (int idx = tid; idx < U.Q_tile * kTcNodes; idx += kTcProducers) {
           const int q = idx / kTcNodes, n = idx % kTcNodes;
-          const float4 r = pn[n];
           float2 e = make_float2(1.f, 0.f);
           if (U.run.factored) {
-            const double c = kq[3 * q] * (double)r.x + kq[3 * q + 1] * (double)r.y + kq[3 * q + 2] * (double)r.z;
-            e = cis_neg_cycles(c);
+            const double4 r = pn[n];
+            e = cis_neg_cycles(kq[3 * q] * r.x + kq[3 * q + 1] * r.y + kq[3 * q + 2] * r.z);
           }
-          etab[idx] = e;
+          et[idx] = e;
         }
         ptx::named_barrier(1, kTcProducers);
         const uint32_t stage = sbase + s * L.stage_bytes;
@@ -374,42 +412,46 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n
           const int h = 2 * half + hh;
           const uint32_t off = kmajor_offset(row, 8 * h, kTcRows);
           if (a_active) {
-            float x[8];
+            uint32_t ah[4], al[4];
 #pragma unroll
             for (int u4 = 0; u4 < 4; ++u4) {
-              const float4 r = pn[4 * h + u4];
-              const double c = kpx * (double)r.x + kpy * (double)r.y + kpz * (double)r.z;
-              float2 e = cis_neg_cycles(c);
-              if (r.w == 0.f) e = make_float2(0.f, 0.f);
-              x[2 * u4] = e.x;
-              x[2 * u4 + 1] = e.y;
+              const int n = 4 * h + u4;
+              const double4 r = pn[n];
+              float2 e = cis_neg_cycles(kpx * r.x + kpy * r.y + kpz * r.z);
+              if (vn[n] == 0.f) e = make_float2(0.f, 0.f);
+              split_pair(e.x, e.y, ah[u4], al[u4]);
             }
-            store_split8(stage + L.a_hi + off, stage + L.a_lo + off, x);
+            ptx::st_shared_v4(stage + L.a_hi + off, ah[0], ah[1], ah[2], ah[3]);
+            ptx::st_shared_v4(stage + L.a_lo + off, al[0], al[1], al[2], al[3]);
           } else {
-            store_zero8(stage + L.a_hi + off, stage + L.a_lo + off);
+            ptx::st_shared_v4(stage + L.a_hi + off, 0u, 0u, 0u, 0u);
+            ptx::st_shared_v4(stage + L.a_lo + off, 0u, 0u, 0u, 0u);
           }
           if (b_rows) {
             const uint32_t o_re = kmajor_offset(2 * row, 8 * h, p.NT);
             const uint32_t o_im = kmajor_offset(2 * row + 1, 8 * h, p.NT);
+            uint32_t rh[4] = {0u, 0u, 0u, 0u}, rl[4] = {0u, 0u, 0u, 0u};
+            uint32_t ih[4] = {0u, 0u, 0u, 0u}, il[4] = {0u, 0u, 0u, 0u};
             if (b_active) {
-              float xr[8], xi[8];
 #pragma unroll
               for (int u4 = 0; u4 < 4; ++u4) {
                 const int n = 4 * h + u4;
-                const float2 e = etab[bq * kTcNodes + n];
+                const float2 e = et[bq * kTcNodes + n];
                 const float2 w = wn[n * p.VG + bv];
                 const float br = e.x * w.x - e.y * w.y, bi = e.x * w.y + e.y * w.x;
-                xr[2 * u4] = br;
-                xr[2 * u4 + 1] = -bi;
-                xi[2 * u4] = bi;
-                xi[2 * u4 + 1] = br;
+                uint32_t hb, lb;
+                split_pair(br, bi, hb, lb);  // (br, bi) halves
+                // row (q,v,re) holds (Re B, -Im B); row (q,v,im) holds (Im B, Re B)
+                rh[u4] = hb ^ 0x80000000u;
+                rl[u4] = lb ^ 0x80000000u;
+                ih[u4] = __byte_perm(hb, 0u, 0x1032);
+                il[u4] = __byte_perm(lb, 0u, 0x1032);
               }
-              store_split8(stage + L.b_hi + o_re, stage + L.b_lo + o_re, xr);
-              store_split8(stage + L.b_hi + o_im, stage + L.b_lo + o_im, xi);
-            } else {
-              store_zero8(stage + L.b_hi + o_re, stage + L.b_lo + o_re);
-              store_zero8(stage + L.b_hi + o_im, stage + L.b_lo + o_im);
             }
+            ptx::st_shared_v4(stage + L.b_hi + o_re, rh[0], rh[1], rh[2], rh[3]);
+            ptx::st_shared_v4(stage + L.b_lo + o_re, rl[0], rl[1], rl[2], rl[3]);
+            ptx::st_shared_v4(stage + L.b_hi + o_im, ih[0], ih[1], ih[2], ih[3]);
+            ptx::st_shared_v4(stage + L.b_lo + o_im, il[0], il[1], il[2], il[3]);
           }
         }
         ptx::fence_proxy_async_smem();
@@ -417,32 +459,28 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n
         // drain the previous group a few stages into the current one, when the
         // MMAs that wrote it have (almost surely) completed
         if (st % kTcDrain == kTcStages - 1 && st / kTcDrain >= 1 && next_drain == st / kTcDrain - 1) {
-          ok = tc_drain(p, U, accfull, accfree, tmem, gbase + next_drain, next_drain == 0, false, ok);
+          tc_drain(p, U, accfull, accfree, tmem, gbase + next_drain, next_drain == 0, false, abort_flag);
           ++next_drain;
-          if (!ok) break;
         }
       }
-      while (ok && next_drain < U.n_groups) {
-        ok = tc_drain(p, U, accfull, accfree, tmem, gbase + next_drain, next_drain == 0,
-                      next_drain == U.n_groups - 1, ok);
+      while (next_drain < U.n_groups) {
+        tc_drain(p, U, accfull, accfree, tmem, gbase + next_drain, next_drain == 0, next_drain == U.n_groups - 1,
+                 abort_flag);
         ++next_drain;
       }
-      if (ok && U.n_groups == 0 && row == tid) {
+      if (U.n_groups == 0 && tid < kTcRows && row < U.P_tile) {
         // no nodes in this split: its share of the tile is zero
         float2 *dst = p.out + (int64_t)U.split * p.S * p.V;
-        if (row < U.P_tile) {
-          const int s_row = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz + U.it.q0 : U.it.p0 + row);
-          for (int q = 0; q < U.Q_tile; ++q)
-            for (int v = 0; v < p.VG; ++v) dst[(int64_t)(s_row + q) * p.V + p.v0 + v] = make_float2(0.f, 0.f);
-        }
+        const int s_row = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz + U.it.q0 : U.it.p0 + row);
+        for (int q = 0; q < U.Q_tile; ++q)
+          for (int v = 0; v < p.VG; ++v) dst[(int64_t)(s_row + q) * p.V + p.v0 + v] = make_float2(0.f, 0.f);
       }
       gbase += U.n_groups;
     }
-    if (!ok) atomicExch(p.error, 1);
   } else if (tid == kTcMmaWarp * 32) {
     // ------------------------------------------------------ MMA issue --
     int gst = 0, gbase = 0;
-    for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
+    for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
       const TcUnit U = tc_unit(p, u);
       for (int st = 0; st < U.n_stages; ++st, ++gst) {
         const int s = gst % kTcStages;
@@ -450,14 +488,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n
         const int gg = gbase + st / kTcDrain;
         const int b = gg & 1;
         const bool group_start = (st % kTcDrain) == 0;
-        if (group_start && gg >= 2 && !ptx::mbar_wait(&accfree[b], ((gg - 2) >> 1) & 1, kTcWaitNs)) {
-          ok = false;
-          break;
-        }
-        if (!ptx::mbar_wait(&full[s], round & 1, kTcWaitNs)) {
-          ok = false;
-          break;
-        }
+        if (group_start && gg >= 2) tc_wait(&accfree[b], ((gg - 2) >> 1) & 1, abort_flag);
+        tc_wait(&full[s], round & 1, abort_flag);
         ptx::tc_fence_after();
         const uint32_t stage = sbase + s * L.stage_bytes;
         const uint32_t acc = tmem + (uint32_t)(b * p.acc_cols);
@@ -478,11 +510,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n
     }
     // all issued MMAs complete before the tensor memory is released
     ptx::mma_commit(done);
-    if (!ptx::mbar_wait(done, 0, kTcWaitNs)) ok = false;
-    if (!ok) atomicExch(p.error, 2);
+    if (!ptx::mbar_wait(done, 0, kTcWaitNs)) *abort_flag = 1;
   }
   ptx::tc_fence_before();
   __syncthreads();
+  if (tid == 0 && *abort_flag) atomicOr(p.error, kErrTimeout);
   if (warp == kTcMmaWarp) {
     ptx::tc_fence_after();
     ptx::tmem_dealloc(tmem, 2 * p.acc_cols);
@@ -496,8 +528,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p, int n
 __global__ void tc_classify_kernel(const float *__restrict__ kx, const float *__restrict__ ky,
                                    const float *__restrict__ kz, const int *__restrict__ start,
                                    const int *__restrict__ counts, int n_lines, int n_kz, TcRun *__restrict__ runs) {
-  const int g = blockIdx.x;
-  if (g >= counts[0]) return;
+  const int n_runs = counts[0];
+  for (int g = blockIdx.x; g < n_runs; g += gridDim.x) {
+  __syncthreads();
   const int s0 = start[g], len = start[g + 1] - s0;
   const int Ls = n_lines * n_kz;
   __shared__ int sep;
@@ -525,15 +558,16 @@ __global__ void tc_classify_kernel(const float *__restrict__ kx, const float *__
     r.Q = sep ? n_kz : 1;
     runs[g] = r;
   }
+  }  // runs
 }
 
 // Item counts per run, factored runs in one list and the rest in another.
 __global__ void tc_count_kernel(const TcRun *__restrict__ runs, const int *__restrict__ counts, int Qt,
-                                int *__restrict__ nf, int *__restrict__ ng) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+                                int *__restrict__ nf, int *__restrict__ ng, int64_t S) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = counts[0];
-  if (g > n) return;
-  if (g == n) {
+  if (g > S) return;
+  if (g >= n) {
     nf[g] = 0;
     ng[g] = 0;
     return;
@@ -570,7 +604,37 @@ __global__ void tc_fill_kernel(const TcRun *__restrict__ runs, int *__restrict__
     }
 }
 
-__global__ void tc_reduce_kernel(const float2 *__restrict__ part, int splits, int64_t count, float2 *__restrict__ out) {
+// Node-range splits: enough work units that the persistent blocks finish
+// together (units per block close to an integer), each split at least 2048
+// nodes; fewer splits win ties.
+__host__ __device__ inline int tc_choose_splits(int64_t items, int64_t N, int max_splits) {
+  if (items <= 0) return 1;
+  int best = 1;
+  double best_eff = -1.0;
+  for (int s = 1; s <= max_splits; ++s) {
+    if (s > 1 && ceil_div(N, s) < 2048) break;
+    const double units = (double)items * s;
+    const double per_block = units / kSmCount;
+    const double eff = per_block / ceil(per_block) * (units < kSmCount ? units / kSmCount : 1.0);
+    if (eff > best_eff + 0.02) {
+      best_eff = eff;
+      best = s;
+    }
+  }
+  return best;
+}
+
+__global__ void tc_plan_kernel(int *__restrict__ counts, int64_t N, int max_splits) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int splits = tc_choose_splits((int64_t)counts[2] + counts[3], N, max_splits);
+  counts[4] = splits;
+  counts[5] = (int)(ceil_div(ceil_div(N, splits), kTcNodes) * kTcNodes);
+}
+
+__global__ void tc_reduce_kernel(const float2 *__restrict__ part, const int *__restrict__ plan, int64_t count,
+                                 float2 *__restrict__ out) {
+  const int splits = plan[4];
+  if (splits <= 1) return;
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   float2 acc = part[e];
@@ -629,26 +693,6 @@ size_t tc_workspace(const fm_signal_args *a) {
   return c.used;
 }
 
-// Node-range splits: enough work units that the persistent blocks finish
-// together (units per block close to an integer), each split at least 2048
-// nodes; fewer splits win ties.
-static int tc_choose_splits(int64_t items, int64_t N, int max_splits) {
-  if (items <= 0) return 1;
-  int best = 1;
-  double best_eff = -1.0;
-  for (int s = 1; s <= max_splits; ++s) {
-    if (s > 1 && ceil_div(N, s) < 2048) break;
-    const double units = (double)items * s;
-    const double per_block = units / kSmCount;
-    const double eff = per_block / std::ceil(per_block) * (units < kSmCount ? units / kSmCount : 1.0);
-    if (eff > best_eff + 0.02) {
-      best_eff = eff;
-      best = s;
-    }
-  }
-  return best;
-}
-
 int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
   const char *who = "fm_signal(BF16X3)";
   cudaStream_t st = ctx->stream;
@@ -665,44 +709,39 @@ int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
     return FM_OK;
   }
   FM_REQUIRE(a->n_lines * a->n_kz < (1LL << 30), FM_ERR_SHAPE, "%s: slab too large", who);
-  FM_TRY(sparse_times_dense<float>(a, pl.csr, static_cast<const float *>(a->Mxy), pl.MM, st));
-  int n_runs = 0, n_tiles = 0;
-  FM_TRY(build_runs<float>(static_cast<const float *>(a->t), S, kTcRows, pl.runs, st, &n_runs, &n_tiles));
-  const MotionDev md = make_motion_dev(a->motion);
-  if (a->motion && a->motion->kind == FM_MOTION_TABLE) {
-    FM_REQUIRE(a->motion->table_calls == n_runs, FM_ERR_SHAPE,
-               "%s: TABLE motion holds %lld entries but t has %d distinct-time runs", who,
-               (long long)a->motion->table_calls, n_runs);
-  }
-  FM_TRY(launch_motion_weights(md, pl.runs.run_t, n_runs, pl.weights, st));
   const float *kx = static_cast<const float *>(a->kx), *ky = static_cast<const float *>(a->ky),
               *kz = static_cast<const float *>(a->kz);
-  tc_classify_kernel<<<n_runs, 256, 0, st>>>(kx, ky, kz, pl.runs.start, pl.runs.counts, (int)a->n_lines,
-                                             (int)a->n_kz, pl.tcruns);
+  FM_TRY(build_runs<float>(static_cast<const float *>(a->t), S, kTcRows, pl.runs, st));
+  FM_TRY(sparse_times_dense<float>(a, pl.csr, static_cast<const float *>(a->Mxy), pl.MM, pl.runs.error, st));
+  FM_TRY(check_table_calls(a->motion, pl.runs, st));
+  const MotionDev md = make_motion_dev(a->motion);
+  FM_TRY(launch_run_weights(md, pl.runs.run_t, pl.runs.counts, S, pl.weights, st));
+  const int64_t cls_blocks = S < 8 * kSmCount ? S : 8 * kSmCount;
+  tc_classify_kernel<<<(unsigned)cls_blocks, 256, 0, st>>>(kx, ky, kz, pl.runs.start, pl.runs.counts,
+                                                           (int)a->n_lines, (int)a->n_kz, pl.tcruns);
   count_launch();
   FM_TRY(check_launch("tc_classify_kernel"));
-  FM_CUDA(cudaMemsetAsync(pl.error, 0, 4 * sizeof(int), st));
 
   for (int64_t v0 = 0; v0 < V; v0 += kTcVGroup) {
     const int VG = (int)((V - v0) < kTcVGroup ? (V - v0) : kTcVGroup);
-    const int Qt_f = (int)((a->n_kz < 128 / VG) ? a->n_kz : (128 / VG > 0 ? 128 / VG : 1));
-    const unsigned gb = (unsigned)ceil_div(n_runs + 1, 256);
-    tc_count_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.nf, pl.ng);
+    // columns per tile: up to 128 (q, v) pairs and at most 64 kz values
+    const int q_cap = (128 / VG < 64) ? 128 / VG : 64;
+    const int Qt_f = (int)((a->n_kz < q_cap) ? a->n_kz : q_cap);
+    const unsigned gb = (unsigned)ceil_div(S + 1, 256);
+    tc_count_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.nf, pl.ng, S);
     count_launch();
     FM_TRY(check_launch("tc_count_kernel"));
     size_t cb = pl.runs.cub_bytes;
-    FM_CUDA(cub::DeviceScan::ExclusiveSum(pl.runs.cub_tmp, cb, pl.nf, pl.of, n_runs + 1, st));
+    FM_CUDA(cub::DeviceScan::ExclusiveSum(pl.runs.cub_tmp, cb, pl.nf, pl.of, (int)(S + 1), st));
     cb = pl.runs.cub_bytes;
-    FM_CUDA(cub::DeviceScan::ExclusiveSum(pl.runs.cub_tmp, cb, pl.ng, pl.og, n_runs + 1, st));
+    FM_CUDA(cub::DeviceScan::ExclusiveSum(pl.runs.cub_tmp, cb, pl.ng, pl.og, (int)(S + 1), st));
     count_launch(2);
     tc_fill_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.of, pl.og, pl.items);
     count_launch();
     FM_TRY(check_launch("tc_fill_kernel"));
-    int h[4] = {0, 0, 0, 0};
-    FM_CUDA(cudaMemcpyAsync(h, pl.runs.counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
-    FM_CUDA(cudaStreamSynchronize(st));
-    const int n_fact = h[2], n_gen = h[3];
-    const int splits = tc_choose_splits(n_fact + n_gen, N, pl.max_splits);
+    tc_plan_kernel<<<1, 32, 0, st>>>(pl.runs.counts, N, pl.max_splits);
+    count_launch();
+    FM_TRY(check_launch("tc_plan_kernel"));
 
     TcDev p{};
     p.N = N; p.S = S; p.V = V;
@@ -720,18 +759,14 @@ int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
     p.run_t = pl.runs.run_t;
     p.runs = pl.tcruns;
     p.items = pl.items;
-    p.splits = splits;
-    p.chunk = ceil_div(ceil_div(N, splits), kTcNodes) * kTcNodes;
-    p.out = (splits > 1) ? pl.partials : out;
+    p.plan = pl.runs.counts;
+    p.partials = pl.partials;
+    p.out = out;
     p.scratch = pl.scratch;
-    p.error = pl.error;
+    p.error = pl.runs.error;
 
     ScopedTimer timer(ctx, "signal_tc");
     for (int kind = 0; kind < 2; ++kind) {
-      const int count = kind == 0 ? n_fact : n_gen;
-      if (count == 0) continue;
-      p.item0 = kind == 0 ? 0 : n_fact;
-      p.n_items = count;
       p.Qt = kind == 0 ? Qt_f : 1;
       const int cols = 2 * p.Qt * VG;
       p.NT = (int)ceil_div(cols, 16) * 16;
@@ -741,24 +776,24 @@ int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
       const size_t smem = Ls.total + 1024;
       FM_REQUIRE(smem <= 232448, FM_ERR_UNSUPPORTED, "%s: tile needs %zu bytes of shared memory", who, smem);
       FM_CUDA(cudaFuncSetAttribute(signal_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      const int n_units = count * splits;
-      const int grid = n_units < kSmCount ? n_units : kSmCount;
-      signal_tc_kernel<<<grid, kTcThreads, smem, st>>>(p, n_units);
+      signal_tc_kernel<<<kSmCount, kTcThreads, smem, st>>>(p, kind);
       count_launch();
       FM_TRY(check_launch("signal_tc_kernel"));
     }
-    if (splits > 1) {
-      const int64_t count = S * V;
-      tc_reduce_kernel<<<(unsigned)ceil_div(count, 256), 256, 0, st>>>(pl.partials, splits, count, out);
-      count_launch();
-      FM_TRY(check_launch("tc_reduce_kernel"));
-    }
+    const int64_t count = S * V;
+    tc_reduce_kernel<<<(unsigned)ceil_div(count, 256), 256, 0, st>>>(pl.partials, pl.runs.counts, count, out);
+    count_launch();
+    FM_TRY(check_launch("tc_reduce_kernel"));
   }
-  int herr = 0;
-  FM_CUDA(cudaMemcpyAsync(&herr, pl.error, sizeof(int), cudaMemcpyDeviceToHost, st));
-  FM_CUDA(cudaStreamSynchronize(st));
-  FM_REQUIRE(herr == 0, FM_ERR_TIMEOUT, "%s: a tensor-core pipeline wait timed out (code %d)", who, herr);
   return FM_OK;
+}
+
+int signal_tc_errors(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
+  Carve cv(ws, ws_bytes);
+  TcPlan pl;
+  carve_tc(cv, a, pl);
+  FM_TRY(carve_ok(cv, "fm_signal(BF16X3)"));
+  return report_errors(pl.runs, ctx->stream, "fm_signal(BF16X3)");
 }
 
 }  // namespace fm

@@ -232,8 +232,10 @@ def signal_args(inp: SignalInputs, motion: LoweredMotion, precision: str, out: t
 
 
 def signal(inp: SignalInputs, motion: LoweredMotion, precision: str = "f32",
-           out: torch.Tensor | None = None) -> torch.Tensor:
-    """k-space (n_ro, n_lines, n_kz, V) of the mass-weighted NUDFT."""
+           out: torch.Tensor | None = None, sync: bool = True, ws: torch.Tensor | None = None) -> torch.Tensor:
+    """k-space (n_ro, n_lines, n_kz, V) of the mass-weighted NUDFT.  With
+    sync=False the work is only queued on the current stream (no host wait);
+    call signal_status with the same inputs and workspace to collect errors."""
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
     dev = inp.r0.device
@@ -241,10 +243,36 @@ def signal(inp: SignalInputs, motion: LoweredMotion, precision: str = "f32",
     if out is None:
         out = torch.empty((*inp.kx.shape, inp.Mxy.shape[1]), dtype=cplx, device=dev)
     a = signal_args(inp, motion, precision, out)
+    if ws is None:
+        ws = workspace(dev, signal_workspace_bytes(a, precision))
+    fn = L.lib().fm_signal if sync else L.lib().fm_signal_enqueue
+    L.check(fn(ctx_for(dev), C.byref(a), PRECISIONS[precision], ws.data_ptr(), ws.numel()))
+    return out
+
+
+def signal_workspace_bytes(a: L.SignalArgs, precision: str) -> int:
     nbytes = C.c_size_t()
     L.check(L.lib().fm_signal_workspace_size(C.byref(a), PRECISIONS[precision], C.byref(nbytes)))
-    ws = workspace(dev, nbytes.value)
-    L.check(L.lib().fm_signal(ctx_for(dev), C.byref(a), PRECISIONS[precision], ws.data_ptr(), ws.numel()))
+    return nbytes.value
+
+
+def signal_status(inp: SignalInputs, motion: LoweredMotion, precision: str, out: torch.Tensor,
+                  ws: torch.Tensor) -> None:
+    """Waits for a queued signal() and raises the errors its device work found."""
+    a = signal_args(inp, motion, precision, out)
+    L.check(L.lib().fm_signal_status(ctx_for(inp.r0.device), C.byref(a), PRECISIONS[precision], ws.data_ptr(),
+                                     ws.numel()))
+
+
+def coil_expand(m: torch.Tensor, sens: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """(N, C) complex64 columns m[n] * sens[n, c] (receive coils)."""
+    dev = m.device
+    N, Cc = sens.shape
+    _check_dev("m", m, torch.complex64, (N,), dev)
+    _check_dev("sens", sens, torch.complex64, (N, Cc), dev)
+    if out is None:
+        out = torch.empty((N, Cc), dtype=torch.complex64, device=dev)
+    L.check(L.lib().fm_coil_expand(ctx_for(dev), m.data_ptr(), sens.data_ptr(), N, Cc, out.data_ptr()))
     return out
 
 

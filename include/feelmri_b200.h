@@ -146,6 +146,11 @@ FM_API int fm_motion_eval(fm_ctx *ctx, const fm_motion *motion, int64_t n_nodes,
 FM_API int fm_motion_eval_workspace_size(const fm_motion *motion, int64_t n_nodes,
                                   int64_t n_times, size_t *bytes);
 
+/* Receive-coil columns: out[n, c] = m[n] * sens[n, c] (complex64), the (N, C)
+ * Mxy that Signal sums per coil.  New component: the reference's Signal
+ * takes no coil sensitivities (cpp/feelmri/MRI.cpp:38-48). */
+FM_API int fm_coil_expand(fm_ctx *ctx, const float *m, const float *sens, int64_t N, int64_t C, float *out);
+
 /* ---- BlochSimulator.solve_mri ------------------------------------------ */
 typedef struct fm_bloch_args {
   int64_t n_pos;           /* N                                             */
@@ -240,6 +245,17 @@ typedef struct fm_signal_args {
  * phase reduced modulo one cycle in FP64). */
 FM_API int fm_signal(fm_ctx *ctx, const fm_signal_args *args, int precision,
               void *workspace, size_t workspace_bytes);
+/* fm_signal in two halves.  fm_signal_enqueue only queues work on the
+ * context's stream: it never waits for the device, so a sequence of calls
+ * can be captured in a CUDA graph or overlapped with other streams.  Errors
+ * found on the device (a sparse row index out of range, a TABLE motion with
+ * the wrong number of entries, a tensor-core wait that ran out) are kept in
+ * the workspace; fm_signal_status waits for the stream and reports them for
+ * the call that used that workspace. */
+FM_API int fm_signal_enqueue(fm_ctx *ctx, const fm_signal_args *args, int precision,
+                             void *workspace, size_t workspace_bytes);
+FM_API int fm_signal_status(fm_ctx *ctx, const fm_signal_args *args, int precision,
+                            void *workspace, size_t workspace_bytes);
 FM_API int fm_signal_workspace_size(const fm_signal_args *args, int precision,
                              size_t *bytes);
 /* Number of distinct-time runs of t (MRI.cpp:109-134 refreshes positions,
