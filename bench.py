@@ -42,10 +42,10 @@ RADIUS, LENGTH = 0.012, 0.1
 VENC = 1.5
 
 
-def build_case(seed: int = 0):
+def build_case(seed: int = 0, n_nodes: int = N_NODES):
     """Host-side synthetic inputs (numpy)."""
     from feelmri_b200 import workloads as W
-    mesh = W.tube(N_NODES, RADIUS, LENGTH)
+    mesh = W.tube(n_nodes, RADIUS, LENGTH)
     N = mesh.n_nodes
     T1, T2 = W.tissue(N, seed)
     phi = W.off_resonance(N, 20.0, seed + 1)
@@ -135,7 +135,7 @@ def run_gpu(args) -> dict | None:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    case = build_case()
+    case = build_case(n_nodes=args.nodes)
     N = case["N"]
     traj = case["traj"]
     S = traj.n_samples
@@ -248,8 +248,8 @@ def run_gpu(args) -> dict | None:
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3" if precision == "bf16x3" else "f32",
             "data": "synthetic (seeded mesh, tissue, flow and trajectory)",
-            "config": {"workload": "phase-contrast flow: 200k-node P1 tube, Poiseuille 1 m/s, 96x96x32 Cartesian, "
-                                   "4 velocity encodings (VENC 1.5 m/s), off-resonance N(0,20 Hz)",
+            "config": {"workload": f"phase-contrast flow: {N // 1000}k-node P1 tube, Poiseuille 1 m/s, "
+                                   "96x96x32 Cartesian, 4 velocity encodings (VENC 1.5 m/s), off-resonance N(0,20 Hz)",
                        "nodes": N, "k_samples": S, "columns": V, "distinct_times": 96,
                        "precision": precision, "l2": "flushed (512 MB write) between timed steps",
                        "parallelism": f"frames x{world}" if world > 1 else "single GPU"},
@@ -385,6 +385,8 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--nodes", type=int, default=N_NODES,
+                    help="mesh size (smaller cases of the same workload for profiling; the metric uses the default)")
     args = ap.parse_args()
     res = run_reference(args) if args.impl == "reference" else run_gpu(args)
     if res is not None:

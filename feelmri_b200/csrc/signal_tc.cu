@@ -43,9 +43,11 @@ constexpr int kTcRows = 128;        // UMMA M
 constexpr int kTcNodes = 16;        // nodes per stage -> K = 32 (two UMMA K steps)
 constexpr int kTcStages = 4;
 constexpr int kTcBlockNodes = 128;  // nodes whose per-run data is formed together
-constexpr int kTcProducers = 256;   // warps 0-7
-constexpr int kTcMmaWarp = 8;
-constexpr int kTcThreads = 288;
+constexpr int kTcStagesPerBlock = kTcBlockNodes / kTcNodes;
+constexpr int kTcProducerWarps = 16;
+constexpr int kTcProducers = 32 * kTcProducerWarps;  // every thread of the block
+constexpr int kTcThreads = kTcProducers;
+constexpr int kTcIssuer = 96;       // thread that issues the MMAs (warp 3: A rows 96-127)
 constexpr int kTcVGroup = 8;        // Mxy columns per launch
 // Stages accumulated in one tensor-memory accumulator before it is drained
 // into an FP32 round-to-nearest running sum.  The tensor core's FP32
@@ -75,10 +77,7 @@ struct TcDev {
   const double *run_t;
   const TcRun *runs;
   const TcItem *items;
-  int item0, n_items;
   int Qt, NT, acc_cols;
-  int splits;
-  int64_t chunk;
   const int *plan;  // device: [2] factored items, [3] generic items, [4] splits, [5] nodes per split
   float2 *partials; // (splits, S, V) when splits > 1
   float2 *out;
@@ -86,9 +85,32 @@ struct TcDev {
   int *error;
 };
 
+// Work list of one launch, read from the device-side plan.
+struct TcWork {
+  int splits, item0, n_items;
+  int64_t chunk;
+  float2 *out;
+};
+
+__device__ inline TcWork tc_work(const TcDev &p, int kind) {
+  TcWork W;
+  W.splits = p.plan[4];
+  W.chunk = p.plan[5];
+  W.item0 = kind == 0 ? 0 : p.plan[2];
+  W.n_items = kind == 0 ? p.plan[2] : p.plan[3];
+  W.out = W.splits > 1 ? p.partials : p.out;
+  return W;
+}
+
+// Shared-memory layout.  Strides of the weight and phase tables are padded
+// (130 and 18 complex values) so that the B producers' 16-byte reads of
+// different columns fall in different banks.
+constexpr int kWStride = kTcBlockNodes + 2;
+constexpr int kEStride = kTcNodes + 2;
+
 struct TcSmem {
   uint32_t stage_bytes, a_hi, a_lo, b_hi, b_lo;  // offsets inside a stage
-  uint32_t posd, valid, w, etab, kq, bars, misc, total;
+  uint32_t pos, w, etab, bars, misc, total;
 };
 
 // Node data is double-buffered: block b is read while block b + 1 is written.
@@ -100,18 +122,14 @@ __host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
   L.b_lo = 2 * kAStageBytes + NT * 2 * kTcNodes * 2;
   L.stage_bytes = 2 * kAStageBytes + 2 * NT * 2 * kTcNodes * 2;
   uint32_t off = kTcStages * L.stage_bytes;
-  L.posd = off;  // [2][128] double4 (x, y, z, unused)
-  off += 2 * kTcBlockNodes * 32;
-  L.valid = off;  // [2][128] float
-  off += 2 * kTcBlockNodes * 4;
-  L.w = off;  // [2][128][VG] float2
-  off += 2 * kTcBlockNodes * VG * 8;
-  L.etab = off;  // [2][Qt][16] float2, by stage parity
-  off += 2 * Qt * kTcNodes * 8;
-  L.kq = off;  // [Qt][3] double
-  off += ((Qt * 24 + 15) / 16) * 16;
+  L.pos = off;  // [2][3][128] double: x, y, z of the moved nodes
+  off += 2 * 3 * kTcBlockNodes * 8;
+  L.w = off;  // [2][VG][kWStride] float2
+  off += 2 * VG * kWStride * 8;
+  L.etab = off;  // [2][Qt][kEStride] float2, by stage parity
+  off += 2 * Qt * kEStride * 8;
   L.bars = off;
-  off += 16 * 8;
+  off += 8 * 8;
   L.misc = off;  // tmem address, abort flag
   off += 16;
   L.total = off;
@@ -122,7 +140,7 @@ __host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
 // `rows` rows and 32 K elements: two K steps of 16, each made of 8-row x
 // 16-byte core matrices (LBO = 128 between K halves, SBO = 256 between row
 // groups).
-__device__ inline uint32_t kmajor_offset(uint32_t row, uint32_t k, uint32_t rows) {
+__host__ __device__ inline uint32_t kmajor_offset(uint32_t row, uint32_t k, uint32_t rows) {
   return (k >> 4) * (rows * 32) + (row >> 3) * 256 + ((k >> 3) & 1) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
@@ -137,15 +155,17 @@ __device__ inline void split_pair(float a, float b, uint32_t &hi, uint32_t &lo) 
   lo = bf16x2_bits(__floats2bfloat162_rn(a - hf.x, b - hf.y));
 }
 
-// exp(-2 pi i c) for c in cycles given in FP64: reduce modulo one with an
-// exact round-to-integer (add/subtract 1.5 * 2^52), then FP32 sin/cos.
-__device__ inline float2 cis_neg_cycles(double c) {
-  const double kRound = 6755399441055744.0;
-  const double n = __dsub_rn(__dadd_rn(c, kRound), kRound);
-  const float f = __double2float_rn(__dsub_rn(c, n));
-  float s, co;
+// cos and sin of 2 pi c for c in cycles given in FP64: c is reduced modulo
+// one exactly (c - rint(c)) before the FP32 sin/cos.
+__device__ inline void cycles_cos_sin(double c, float &co, float &s) {
+  const float f = __double2float_rn(__dsub_rn(c, rint(c)));
   __sincosf(6.283185307179586f * f, &s, &co);
-  return make_float2(co, -s);
+}
+
+__device__ inline void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  // no memory clobber: the stores are ordered before the proxy fence (also
+  // volatile) that publishes them, and no generic load reads them back
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d));
 }
 
 struct TcUnit {
@@ -155,16 +175,16 @@ struct TcUnit {
   int64_t n_begin, n_end;
 };
 
-__device__ inline TcUnit tc_unit(const TcDev &p, int u) {
+__device__ inline TcUnit tc_unit(const TcDev &p, const TcWork &W, int u) {
   TcUnit U;
-  const int item = u % p.n_items;
-  U.split = u / p.n_items;
-  U.it = p.items[p.item0 + item];
+  const int item = u % W.n_items;
+  U.split = u / W.n_items;
+  U.it = p.items[W.item0 + item];
   U.run = p.runs[U.it.run];
   U.P_tile = min(kTcRows, U.run.P - U.it.p0);
   U.Q_tile = min(p.Qt, U.run.Q - U.it.q0);
-  U.n_begin = (int64_t)U.split * p.chunk;
-  U.n_end = min(p.N, U.n_begin + p.chunk);
+  U.n_begin = (int64_t)U.split * W.chunk;
+  U.n_end = min(p.N, U.n_begin + W.chunk);
   U.n_stages = U.n_end > U.n_begin ? (int)ceil_div(U.n_end - U.n_begin, kTcNodes) : 0;
   U.n_groups = (int)ceil_div(U.n_stages, kTcDrain);
   return U;
@@ -179,8 +199,11 @@ __device__ inline bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abo
   return false;
 }
 
-// Raw node data loaded one node block ahead (global loads in flight while
-// the current block is processed).
+__device__ inline void prefetch_l1(const void *ptr) { asm volatile("prefetch.global.L1 [%0];" ::"l"(ptr)); }
+
+// Raw node data loaded two stages before it is derived (global loads in
+// flight meanwhile); the node's POD mode rows are prefetched into L1 for the
+// displacement.
 struct TcRaw {
   float x, y, z, t2, phi;
   float2 m[kTcVGroup];
@@ -195,13 +218,23 @@ __device__ inline void tc_load_raw(const TcDev &p, int64_t n, TcRaw &r) {
 #pragma unroll
   for (int v = 0; v < kTcVGroup; ++v)
     if (v < p.VG) r.m[v] = p.MM[n * p.V + p.v0 + v];
+  if (p.md.kind == FM_MOTION_TERMS) {
+    for (int k = 0; k < p.md.n_terms; ++k) {
+      const fm_motion_term &T = p.md.terms[k];
+      if (T.kind == FM_TERM_RESPIRATORY) continue;
+      const float *Phi = T.modes + (size_t)n * 3 * T.n_modes;
+      prefetch_l1(Phi);
+      prefetch_l1(Phi + 3 * T.n_modes - 1);
+    }
+  }
 }
 
-// Per-run node quantities of one node into buffer `buf`: moved position (in
-// FP64 for the phase products), validity and the decayed, off-resonance
-// rotated weights W' = (M Mxy)[n, v] exp(-t / T2) exp(i phi t).
+// Per-run node quantities of one node into slot `slot` of a node buffer:
+// moved position (in FP64 for the phase products) and the decayed,
+// off-resonance rotated weights W' = (M Mxy)[n, v] exp(-t / T2) exp(i phi t).
+// Nodes past the range get position 0 and zero weights, so they add nothing.
 __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, const TcRaw &r, const float *wrun,
-                                 float tg, double4 *posd, float *valid, float2 *wblk, int slot) {
+                                 float tg, double *pos, float2 *wblk, int slot) {
   if (n < U.n_end) {
     float x = r.x, y = r.y, z = r.z;
     if (p.md.kind == FM_MOTION_TERMS) {
@@ -212,302 +245,358 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
       const float *d = p.table + ((int64_t)U.it.run * p.N + n) * 3;
       x = x + d[0]; y = y + d[1]; z = z + d[2];
     }
-    posd[slot] = make_double4((double)x, (double)y, (double)z, 0.0);
-    valid[slot] = 1.f;
+    pos[slot] = (double)x;
+    pos[kTcBlockNodes + slot] = (double)y;
+    pos[2 * kTcBlockNodes + slot] = (double)z;
     const float decay = expf(-tg * (1.0f / r.t2));
     float so, co;
     sincosf(r.phi * tg, &so, &co);
     const float er = decay * co, ei = decay * so;
 #pragma unroll
     for (int v = 0; v < kTcVGroup; ++v)
-      if (v < p.VG) wblk[slot * p.VG + v] = make_float2(r.m[v].x * er - r.m[v].y * ei, r.m[v].x * ei + r.m[v].y * er);
+      if (v < p.VG)
+        wblk[v * kWStride + slot] = make_float2(r.m[v].x * er - r.m[v].y * ei, r.m[v].x * ei + r.m[v].y * er);
   } else {
-    posd[slot] = make_double4(0.0, 0.0, 0.0, 0.0);
-    valid[slot] = 0.f;
-    for (int v = 0; v < p.VG; ++v) wblk[slot * p.VG + v] = make_float2(0.f, 0.f);
+    pos[slot] = 0.0;
+    pos[kTcBlockNodes + slot] = 0.0;
+    pos[2 * kTcBlockNodes + slot] = 0.0;
+    for (int v = 0; v < p.VG; ++v) wblk[v * kWStride + slot] = make_float2(0.f, 0.f);
   }
+}
+
+// Phase table of one stage of a factored unit: e_q(n) = exp(-2 pi i kq_q . r_n)
+// for q = q0 (and q0 + 32) and the two nodes n0, n0 + 1 of this thread.
+__device__ inline void tc_phase_pair(const double *pb, float2 *et, int q, int n0, double kx, double ky, double kz) {
+  const double2 x = *reinterpret_cast<const double2 *>(pb + n0);
+  const double2 y = *reinterpret_cast<const double2 *>(pb + kTcBlockNodes + n0);
+  const double2 z = *reinterpret_cast<const double2 *>(pb + 2 * kTcBlockNodes + n0);
+  float c0, s0, c1, s1;
+  cycles_cos_sin(fma(kz, z.x, fma(ky, y.x, kx * x.x)), c0, s0);
+  cycles_cos_sin(fma(kz, z.y, fma(ky, y.y, kx * x.y)), c1, s1);
+  *reinterpret_cast<float4 *>(et + q * kEStride + n0) = make_float4(c0, -s0, c1, -s1);
 }
 
 // Adds accumulator `b` (one drained group) into the block's running sums,
 // or, for the unit's last group, writes running sums + accumulator to the
-// output samples.  Executed by all 256 producers: warp w reads TMEM lanes of
-// quarter w % 4 and column half w / 4.
-__device__ inline void tc_drain(const TcDev &p, const TcUnit &U, uint64_t *accfull, uint64_t *accfree, uint32_t tmem,
+// output samples.  Accumulator columns: pair j's real part in column j, its
+// imaginary part in column NT/2 + j.  Warp w reads TMEM lanes of quarter
+// w % 4 and every fourth chunk of 8 pairs starting at w / 4.
+__device__ inline void tc_drain(const TcDev &p, const TcWork &W, const TcUnit &U, uint64_t *accfull, uint32_t tmem,
                                 int gg, bool first, bool final, volatile int *abort_flag) {
   const int tid = threadIdx.x, warp = tid >> 5;
   const int b = gg & 1;
   tc_wait(&accfull[b], (gg >> 1) & 1, abort_flag);
   ptx::tc_fence_after();
-  const int quarter = warp & 3, half = warp >> 2;
+  const int quarter = warp & 3;
   const int row = quarter * 32 + (tid & 31);
-  const int cph = ((p.NT / 2 + 15) / 16) * 16;
-  const int c_begin = half * cph, c_end = min(p.NT, c_begin + cph);
+  const int NH = p.NT >> 1;
   float *srow = p.scratch + ((size_t)blockIdx.x * kTcRows + row) * p.NT;
   const bool row_ok = row < U.P_tile;
-  float2 *dst = p.out + (int64_t)U.split * p.S * p.V;
+  float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
   const int s_row = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz + U.it.q0 : U.it.p0 + row);
-  for (int c0 = c_begin; c0 < c_end; c0 += 16) {
-    uint32_t r[16];
-    ptx::tmem_ld16(tmem + (uint32_t)(b * p.acc_cols) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, r);
+  const uint32_t taddr = tmem + (uint32_t)(b * p.acc_cols) + ((uint32_t)(quarter * 32) << 16);
+  for (int c0 = (warp >> 2) * 8; c0 < NH; c0 += 32) {
+    // running sums first, so their loads overlap the tensor-memory reads
+    float4 re0 = make_float4(0.f, 0.f, 0.f, 0.f), re1 = re0, im0 = re0, im1 = re0;
+    if (!first && row_ok) {
+      re0 = *reinterpret_cast<const float4 *>(srow + c0);
+      re1 = *reinterpret_cast<const float4 *>(srow + c0 + 4);
+      im0 = *reinterpret_cast<const float4 *>(srow + NH + c0);
+      im1 = *reinterpret_cast<const float4 *>(srow + NH + c0 + 4);
+    }
+    uint32_t r[8], m[8];
+    ptx::tmem_ld8(taddr + (uint32_t)c0, r);
+    ptx::tmem_ld8(taddr + (uint32_t)(NH + c0), m);
     ptx::tmem_wait_ld();
     if (!row_ok) continue;
-    float v[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-    if (!first) {
-      const float4 *src = reinterpret_cast<const float4 *>(srow + c0);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const float4 a = src[i];
-        v[4 * i] += a.x; v[4 * i + 1] += a.y; v[4 * i + 2] += a.z; v[4 * i + 3] += a.w;
-      }
-    }
+    re0.x += __uint_as_float(r[0]); re0.y += __uint_as_float(r[1]); re0.z += __uint_as_float(r[2]);
+    re0.w += __uint_as_float(r[3]); re1.x += __uint_as_float(r[4]); re1.y += __uint_as_float(r[5]);
+    re1.z += __uint_as_float(r[6]); re1.w += __uint_as_float(r[7]);
+    im0.x += __uint_as_float(m[0]); im0.y += __uint_as_float(m[1]); im0.z += __uint_as_float(m[2]);
+    im0.w += __uint_as_float(m[3]); im1.x += __uint_as_float(m[4]); im1.y += __uint_as_float(m[5]);
+    im1.z += __uint_as_float(m[6]); im1.w += __uint_as_float(m[7]);
     if (!final) {
-      float4 *d4 = reinterpret_cast<float4 *>(srow + c0);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) d4[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+      *reinterpret_cast<float4 *>(srow + c0) = re0;
+      *reinterpret_cast<float4 *>(srow + c0 + 4) = re1;
+      *reinterpret_cast<float4 *>(srow + NH + c0) = im0;
+      *reinterpret_cast<float4 *>(srow + NH + c0 + 4) = im1;
     } else {
+      const float rv[8] = {re0.x, re0.y, re0.z, re0.w, re1.x, re1.y, re1.z, re1.w};
+      const float iv[8] = {im0.x, im0.y, im0.z, im0.w, im1.x, im1.y, im1.z, im1.w};
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        const int jj = (c0 >> 1) + i;
+        const int jj = c0 + i;  // pair (q, v)
         const int q = jj / p.VG, vv = jj % p.VG;
-        if (q < U.Q_tile) dst[(int64_t)(s_row + q) * p.V + p.v0 + vv] = make_float2(v[2 * i], v[2 * i + 1]);
+        if (q < U.Q_tile) dst[(int64_t)(s_row + q) * p.V + p.v0 + vv] = make_float2(rv[i], iv[i]);
       }
     }
   }
+  // the next MMA into this accumulator is issued after a block barrier
   ptx::tc_fence_before();
-  ptx::mbar_arrive(&accfree[b]);
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p_in, int kind) {
+// MMAs of one stage (global stage index g, stage-local st of a unit with
+// n_stages stages, accumulator group gg): A_hi B_hi + A_hi B_lo + A_lo B_hi
+// over the two K steps; the stage's shared memory is released by a commit to
+// empty[s], and the group's accumulator by a commit to accfull[gg & 1] after
+// its last stage.
+__device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, uint32_t idesc, int NT,
+                                int acc_cols, uint64_t *empty, uint64_t *accfull, int g, int st, int n_stages,
+                                int gg) {
+  const int s = g % kTcStages;
+  const int b = gg & 1;
+  const bool group_start = (st % kTcDrain) == 0;
+  ptx::tc_fence_after();
+  const uint32_t stage = sbase + s * L.stage_bytes;
+  const uint32_t acc = tmem + (uint32_t)(b * acc_cols);
+#pragma unroll
+  for (int ks = 0; ks < 2; ++ks) {
+    const uint64_t ah = ptx::smem_desc(stage + L.a_hi + ks * kTcRows * 32, 128, 256);
+    const uint64_t al = ptx::smem_desc(stage + L.a_lo + ks * kTcRows * 32, 128, 256);
+    const uint64_t bh = ptx::smem_desc(stage + L.b_hi + ks * NT * 32, 128, 256);
+    const uint64_t bl = ptx::smem_desc(stage + L.b_lo + ks * NT * 32, 128, 256);
+    ptx::mma_bf16(acc, ah, bh, idesc, (group_start && ks == 0) ? 0u : 1u);
+    ptx::mma_bf16(acc, ah, bl, idesc, 1u);
+    ptx::mma_bf16(acc, al, bh, idesc, 1u);
+  }
+  ptx::mma_commit(&empty[s]);
+  if ((st % kTcDrain) == kTcDrain - 1 || st == n_stages - 1) ptx::mma_commit(&accfull[b]);
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_constant__ TcDev p, int kind) {
   extern __shared__ __align__(1024) unsigned char smem[];
   // work sizes come from the device-side plan, so the launch needs no host
   // synchronisation (and can be captured in a CUDA graph)
-  TcDev p = p_in;
-  p.splits = p_in.plan[4];
-  p.chunk = p_in.plan[5];
-  p.item0 = kind == 0 ? 0 : p_in.plan[2];
-  p.n_items = kind == 0 ? p_in.plan[2] : p_in.plan[3];
-  p.out = p.splits > 1 ? p_in.partials : p_in.out;
-  const int n_units = p.n_items * p.splits;
+  const TcWork W = tc_work(p, kind);
+  const int n_units = W.n_items * W.splits;
   const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  const TcSmem L = tc_smem_layout(p.NT, p.VG, p.Qt);
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + L.bars);
-  uint64_t *empty = full + kTcStages;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int NT = p.NT, NH = NT >> 1, VG = p.VG, Qt = p.Qt;
+  const TcSmem L = tc_smem_layout(NT, VG, Qt);
+  uint64_t *empty = reinterpret_cast<uint64_t *>(smem + L.bars);
   uint64_t *accfull = empty + kTcStages;
-  uint64_t *accfree = accfull + 2;
-  uint64_t *done = accfree + 2;
+  uint64_t *done = accfull + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L.misc);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + L.misc + 4);
-  double4 *posd_all = reinterpret_cast<double4 *>(smem + L.posd);
-  float *valid_all = reinterpret_cast<float *>(smem + L.valid);
+  double *pos_all = reinterpret_cast<double *>(smem + L.pos);
   float2 *w_all = reinterpret_cast<float2 *>(smem + L.w);
   float2 *etab = reinterpret_cast<float2 *>(smem + L.etab);
-  double *kq = reinterpret_cast<double *>(smem + L.kq);
   const uint32_t sbase = ptx::smem_addr(smem);
 
   if (tid == 0) {
-    for (int s = 0; s < kTcStages; ++s) {
-      ptx::mbar_init(&full[s], kTcProducers);
-      ptx::mbar_init(&empty[s], 1);
-    }
-    for (int b = 0; b < 2; ++b) {
-      ptx::mbar_init(&accfull[b], 1);
-      ptx::mbar_init(&accfree[b], kTcProducers);
-    }
+    for (int s = 0; s < kTcStages; ++s) ptx::mbar_init(&empty[s], 1);
+    for (int b = 0; b < 2; ++b) ptx::mbar_init(&accfull[b], 1);
     ptx::mbar_init(done, 1);
     *abort_flag = 0;
     ptx::fence_mbar_init();
   }
-  if (warp == kTcMmaWarp) ptx::tmem_alloc(tmem_slot, 2 * p.acc_cols);
+  if (warp == 0) ptx::tmem_alloc(tmem_slot, 2 * p.acc_cols);
   ptx::tc_fence_before();
   __syncthreads();
   ptx::tc_fence_after();
   const uint32_t tmem = tmem_slot[0];
-  const uint32_t idesc = ptx::idesc_bf16_f32(kTcRows, p.NT);
+  const uint32_t idesc = ptx::idesc_bf16_f32(kTcRows, NT);
 
-  if (warp < kTcMmaWarp) {
-    // ------------------------------------------------------ producers --
-    const int row = tid & (kTcRows - 1);  // A row / B (q, v) pair of this thread
-    const int half = tid >> 7;            // which 8 of the 16 nodes of a stage
-    const bool loader = tid < kTcBlockNodes;
-    int gst = 0, gbase = 0;
-    TcRaw raw;
-    for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
-      const TcUnit U = tc_unit(p, u);
-      ptx::named_barrier(1, kTcProducers);  // the previous unit's readers are done
-      for (int q = tid; q < U.Q_tile; q += kTcProducers) {
-        const int s_q = U.run.start + U.it.q0 + q, s_0 = U.run.start;
-        kq[3 * q + 0] = U.run.factored ? (double)p.kx[s_q] - (double)p.kx[s_0] : 0.0;
-        kq[3 * q + 1] = U.run.factored ? (double)p.ky[s_q] - (double)p.ky[s_0] : 0.0;
-        kq[3 * q + 2] = U.run.factored ? (double)p.kz[s_q] - (double)p.kz[s_0] : 0.0;
+  // Roles (warp-uniform).  Warps 0-7 write A: rows 32 (w >> 1) + lane, nodes
+  // 8 (w & 1) .. + 7 of every stage.  Warps 8-15 write B: pairs
+  // 32 ((w - 8) >> 1) + lane, same node halves, and the next stage's phase
+  // table.  Threads 0-127 also derive the node blocks.  One thread of warp 7
+  // issues a stage's MMAs after the block barrier that follows the stage
+  // (every writer has fenced its stores to the async proxy by then).
+  const bool a_role = warp < 8;
+  const int rw = a_role ? warp : warp - 8;
+  const int row = (rw >> 1) * 32 + lane;  // A row or B pair
+  const int half = rw & 1;                // nodes 8 half .. 8 half + 7 of a stage
+  const bool loader = tid < kTcBlockNodes;
+  const bool issuer = tid == 7 * 32;
+  // operand addresses inside a stage (K chunk 2 half and 2 half + 1 of 8)
+  const uint32_t a0 = kmajor_offset(row, 16 * half, kTcRows), a1 = kmajor_offset(row, 16 * half + 8, kTcRows);
+  const bool b_rows = row < NH;
+  const uint32_t re0 = kmajor_offset(row, 16 * half, NT), re1 = kmajor_offset(row, 16 * half + 8, NT);
+  const uint32_t im0 = kmajor_offset(NH + row, 16 * half, NT), im1 = kmajor_offset(NH + row, 16 * half + 8, NT);
+  // phase-table thread: q = (tid - 256) / 8 (+ 32), nodes 2 ((tid - 256) % 8) + {0, 1}
+  const int tq = (tid - 256) >> 3, tn = ((tid - 256) & 7) * 2;
+  int gst = 0, gbase = 0;
+  TcRaw raw;
+  for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
+    const TcUnit U = tc_unit(p, W, u);
+    const bool fac = U.run.factored != 0;
+    ptx::named_barrier(1, kTcProducers);  // the previous unit's readers are done
+    // per-unit row data in registers
+    double kx0 = 0, ky0 = 0, kz0 = 0, kx1 = 0, ky1 = 0, kz1 = 0;  // A: kp of the row; B: kq of q and q + 32
+    int bq = 0, bv = 0;
+    const bool a_warp_active = a_role && (rw >> 1) * 32 < U.P_tile;
+    if (a_role) {
+      if (row < U.P_tile) {
+        const int s_p = U.run.start + (fac ? (U.it.p0 + row) * p.n_kz : U.it.p0 + row);
+        kx0 = p.kx[s_p];
+        ky0 = p.ky[s_p];
+        kz0 = p.kz[s_p];
       }
-      const bool a_active = row < U.P_tile;
-      double kpx = 0, kpy = 0, kpz = 0;
-      if (a_active) {
-        const int s_p = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz : U.it.p0 + row);
-        kpx = p.kx[s_p];
-        kpy = p.ky[s_p];
-        kpz = p.kz[s_p];
+    } else {
+      if (row < U.Q_tile * VG) {
+        bq = row / VG;
+        bv = row % VG;
       }
-      const bool b_rows = 2 * row < p.NT;
-      const bool b_active = row < U.Q_tile * p.VG;
-      const int bq = b_active ? row / p.VG : 0, bv = b_active ? row % p.VG : 0;
-      const float *wrun = p.weights ? p.weights + (int64_t)U.it.run * p.md.slots : nullptr;
-      const float tg = (float)p.run_t[U.it.run];
-      const int n_blocks = (int)ceil_div(U.n_stages, kTcBlockNodes / kTcNodes);
-      // prologue: node block 0 into buffer 0, block 1's loads in flight
-      if (loader && U.n_stages > 0) {
-        const int64_t n = U.n_begin + tid;
-        if (n < U.n_end) tc_load_raw(p, n, raw);
-        tc_derive(p, U, n, raw, wrun, tg, posd_all, valid_all, w_all, tid);
-        const int64_t n1 = n + kTcBlockNodes;
-        if (n_blocks > 1 && n1 < U.n_end) tc_load_raw(p, n1, raw);
+      if (fac) {
+        const int s_0 = U.run.start;
+        if (tq < U.Q_tile) {
+          const int s_q = U.run.start + U.it.q0 + tq;
+          kx0 = (double)p.kx[s_q] - (double)p.kx[s_0];
+          ky0 = (double)p.ky[s_q] - (double)p.ky[s_0];
+          kz0 = (double)p.kz[s_q] - (double)p.kz[s_0];
+        }
+        if (tq + 32 < U.Q_tile) {
+          const int s_q = U.run.start + U.it.q0 + tq + 32;
+          kx1 = (double)p.kx[s_q] - (double)p.kx[s_0];
+          ky1 = (double)p.ky[s_q] - (double)p.ky[s_0];
+          kz1 = (double)p.kz[s_q] - (double)p.kz[s_0];
+        }
       }
-      int next_drain = 0;
+    }
+    const bool t_on0 = !a_role && fac && tq < U.Q_tile, t_on1 = !a_role && fac && tq + 32 < U.Q_tile;
+    const float *wrun = p.weights ? p.weights + (int64_t)U.it.run * p.md.slots : nullptr;
+    const float tg = (float)p.run_t[U.it.run];
+    const int n_blocks = (int)ceil_div(U.n_stages, kTcStagesPerBlock);
+    // prologue: node block 0 into buffer 0
+    if (loader && U.n_stages > 0) {
+      const int64_t n = U.n_begin + tid;
+      if (n < U.n_end) tc_load_raw(p, n, raw);
+      tc_derive(p, U, n, raw, wrun, tg, pos_all, w_all, tid);
+    }
+    ptx::named_barrier(1, kTcProducers);  // block 0 is visible
+    if (U.n_stages > 0) {
+      if (t_on0) tc_phase_pair(pos_all, etab, tq, tn, kx0, ky0, kz0);
+      if (t_on1) tc_phase_pair(pos_all, etab, tq + 32, tn, kx1, ky1, kz1);
+    }
+    int next_drain = 0;
 
-      for (int st = 0; st < U.n_stages; ++st, ++gst) {
-        const int s = gst % kTcStages;
-        const uint32_t round = gst / kTcStages;
-        const int j = st % (kTcBlockNodes / kTcNodes);
-        const int blk = st / (kTcBlockNodes / kTcNodes);
-        const int buf = blk & 1;
-        if (j == 0) {
-          // buffer `buf` (written during the previous block) is complete, and
-          // every producer is done with the other buffer
-          ptx::named_barrier(1, kTcProducers);
-          if (loader && blk >= 1 && blk + 1 < n_blocks) {
-            const int64_t n2 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes + tid;
-            if (n2 < U.n_end) tc_load_raw(p, n2, raw);
-          }
-        }
-        if (j == 4 && loader && blk + 1 < n_blocks) {
-          const int64_t n1 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes + tid;
-          tc_derive(p, U, n1, raw, wrun, tg, posd_all + (buf ^ 1) * kTcBlockNodes,
-                    valid_all + (buf ^ 1) * kTcBlockNodes, w_all + (buf ^ 1) * kTcBlockNodes * p.VG, tid);
-        }
-        const double4 *pn = posd_all + buf * kTcBlockNodes + j * kTcNodes;
-        const float *vn = valid_all + buf * kTcBlockNodes + j * kTcNodes;
-        const float2 *wn = w_all + (buf * kTcBlockNodes + j * kTcNodes) * p.VG;
-        // wait until the MMAs that last read stage s are done
-        tc_wait(&empty[s], (round & 1) ^ 1, abort_flag);
-        // e_q(n) = exp(-2 pi i kq_q . r_n) for this stage's nodes.  Buffers
-        // alternate by stage: a thread that writes stage st's table has passed
-        // the barrier of stage st - 1, so every reader of stage st - 2 is done.
-        float2 *et = etab + (st & 1) * p.Qt * kTcNodes;
-        for (int idx = tid; idx < U.Q_tile * kTcNodes; idx += kTcProducers) {
-          const int q = idx / kTcNodes, n = idx % kTcNodes;
-          float2 e = make_float2(1.f, 0.f);
-          if (U.run.factored) {
-            const double4 r = pn[n];
-            e = cis_neg_cycles(kq[3 * q] * r.x + kq[3 * q + 1] * r.y + kq[3 * q + 2] * r.z);
-          }
-          et[idx] = e;
-        }
-        ptx::named_barrier(1, kTcProducers);
-        const uint32_t stage = sbase + s * L.stage_bytes;
+    for (int st = 0; st < U.n_stages; ++st, ++gst) {
+      const int s = gst & (kTcStages - 1);
+      const uint32_t round = (uint32_t)gst / kTcStages;
+      const int j = st & (kTcStagesPerBlock - 1);
+      const int blk = st / kTcStagesPerBlock;
+      const int buf = blk & 1;
+      if (loader && blk + 1 < n_blocks) {
+        // block blk + 1 (block blk is then complete): raw loads issued at
+        // j == 4, derived into the other buffer at j == 6.  That buffer's
+        // readers (stages of block blk - 1) passed this block's first barrier.
+        const int64_t n1 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes + tid;
+        if (j == 4 && n1 < U.n_end) tc_load_raw(p, n1, raw);
+        if (j == 6)
+          tc_derive(p, U, n1, raw, wrun, tg, pos_all + (buf ^ 1) * 3 * kTcBlockNodes,
+                    w_all + (buf ^ 1) * VG * kWStride, tid);
+      }
+      // wait until the MMAs that last read stage s are done
+      tc_wait(&empty[s], (round & 1) ^ 1, abort_flag);
+      // every writer of the previous stage is done (its MMAs go out now); the
+      // phase table of this stage and the node blocks derived up to the
+      // previous stage are visible
+      ptx::named_barrier(1, kTcProducers);
+      if (issuer && st > 0)
+        tc_issue(L, sbase, tmem, idesc, NT, p.acc_cols, empty, accfull, gst - 1, st - 1, U.n_stages,
+                 gbase + (st - 1) / kTcDrain);
+      const uint32_t stg = sbase + s * L.stage_bytes;
+      const int nb = j * kTcNodes + 8 * half;  // first node of this thread in the block
+      if (a_warp_active) {
+        // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n
+        const double *px = pos_all + buf * 3 * kTcBlockNodes + nb;
+        uint32_t h[8], l[8];
 #pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {  // two chunks of 4 nodes (8 K values)
-          const int h = 2 * half + hh;
-          const uint32_t off = kmajor_offset(row, 8 * h, kTcRows);
-          if (a_active) {
-            uint32_t ah[4], al[4];
+        for (int u4 = 0; u4 < 8; u4 += 2) {
+          const double2 x = *reinterpret_cast<const double2 *>(px + u4);
+          const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
+          const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
+          float c0, s0, c1, s1;
+          cycles_cos_sin(fma(kz0, z.x, fma(ky0, y.x, kx0 * x.x)), c0, s0);
+          cycles_cos_sin(fma(kz0, z.y, fma(ky0, y.y, kx0 * x.y)), c1, s1);
+          split_pair(c0, s0, h[u4], l[u4]);
+          split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
+        }
+        st_shared_v4(stg + L.a_hi + a0, h[0], h[1], h[2], h[3]);
+        st_shared_v4(stg + L.a_hi + a1, h[4], h[5], h[6], h[7]);
+        st_shared_v4(stg + L.a_lo + a0, l[0], l[1], l[2], l[3]);
+        st_shared_v4(stg + L.a_lo + a1, l[4], l[5], l[6], l[7]);
+      } else if (!a_role) {
+        // B'^T rows: re row `row` = (Re B, Im B), im row NT/2 + row =
+        // (Im B, -Re B), B = e_q(n) W'(n, v).  Pairs past Q_tile VG hold
+        // values no output reads.
+        const float4 *wp = reinterpret_cast<const float4 *>(w_all + (buf * VG + bv) * kWStride + nb);
+        float br[8], bi[8];
 #pragma unroll
-            for (int u4 = 0; u4 < 4; ++u4) {
-              const int n = 4 * h + u4;
-              const double4 r = pn[n];
-              float2 e = cis_neg_cycles(kpx * r.x + kpy * r.y + kpz * r.z);
-              if (vn[n] == 0.f) e = make_float2(0.f, 0.f);
-              split_pair(e.x, e.y, ah[u4], al[u4]);
-            }
-            ptx::st_shared_v4(stage + L.a_hi + off, ah[0], ah[1], ah[2], ah[3]);
-            ptx::st_shared_v4(stage + L.a_lo + off, al[0], al[1], al[2], al[3]);
-          } else {
-            ptx::st_shared_v4(stage + L.a_hi + off, 0u, 0u, 0u, 0u);
-            ptx::st_shared_v4(stage + L.a_lo + off, 0u, 0u, 0u, 0u);
-          }
-          if (b_rows) {
-            const uint32_t o_re = kmajor_offset(2 * row, 8 * h, p.NT);
-            const uint32_t o_im = kmajor_offset(2 * row + 1, 8 * h, p.NT);
-            uint32_t rh[4] = {0u, 0u, 0u, 0u}, rl[4] = {0u, 0u, 0u, 0u};
-            uint32_t ih[4] = {0u, 0u, 0u, 0u}, il[4] = {0u, 0u, 0u, 0u};
-            if (b_active) {
+        for (int i = 0; i < 4; ++i) {
+          const float4 w2 = wp[i];
+          br[2 * i] = w2.x; bi[2 * i] = w2.y; br[2 * i + 1] = w2.z; bi[2 * i + 1] = w2.w;
+        }
+        if (fac) {
+          const float4 *ep = reinterpret_cast<const float4 *>(etab + ((st & 1) * Qt + bq) * kEStride + nb - j * kTcNodes);
 #pragma unroll
-              for (int u4 = 0; u4 < 4; ++u4) {
-                const int n = 4 * h + u4;
-                const float2 e = et[bq * kTcNodes + n];
-                const float2 w = wn[n * p.VG + bv];
-                const float br = e.x * w.x - e.y * w.y, bi = e.x * w.y + e.y * w.x;
-                uint32_t hb, lb;
-                split_pair(br, bi, hb, lb);  // (br, bi) halves
-                // row (q,v,re) holds (Re B, -Im B); row (q,v,im) holds (Im B, Re B)
-                rh[u4] = hb ^ 0x80000000u;
-                rl[u4] = lb ^ 0x80000000u;
-                ih[u4] = __byte_perm(hb, 0u, 0x1032);
-                il[u4] = __byte_perm(lb, 0u, 0x1032);
-              }
-            }
-            ptx::st_shared_v4(stage + L.b_hi + o_re, rh[0], rh[1], rh[2], rh[3]);
-            ptx::st_shared_v4(stage + L.b_lo + o_re, rl[0], rl[1], rl[2], rl[3]);
-            ptx::st_shared_v4(stage + L.b_hi + o_im, ih[0], ih[1], ih[2], ih[3]);
-            ptx::st_shared_v4(stage + L.b_lo + o_im, il[0], il[1], il[2], il[3]);
+          for (int i = 0; i < 4; ++i) {
+            const float4 e2 = ep[i];
+            const float wr0 = br[2 * i], wi0 = bi[2 * i], wr1 = br[2 * i + 1], wi1 = bi[2 * i + 1];
+            br[2 * i] = e2.x * wr0 - e2.y * wi0;
+            bi[2 * i] = e2.x * wi0 + e2.y * wr0;
+            br[2 * i + 1] = e2.z * wr1 - e2.w * wi1;
+            bi[2 * i + 1] = e2.z * wi1 + e2.w * wr1;
           }
         }
-        ptx::fence_proxy_async_smem();
-        ptx::mbar_arrive(&full[s]);
-        // drain the previous group a few stages into the current one, when the
-        // MMAs that wrote it have (almost surely) completed
-        if (st % kTcDrain == kTcStages - 1 && st / kTcDrain >= 1 && next_drain == st / kTcDrain - 1) {
-          tc_drain(p, U, accfull, accfree, tmem, gbase + next_drain, next_drain == 0, false, abort_flag);
-          ++next_drain;
+        uint32_t hr[8], lr[8], hm[8], lm[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          split_pair(br[i], bi[i], hr[i], lr[i]);
+          hm[i] = __byte_perm(hr[i], 0u, 0x1032) ^ 0x80000000u;
+          lm[i] = __byte_perm(lr[i], 0u, 0x1032) ^ 0x80000000u;
+        }
+        if (b_rows) {
+          st_shared_v4(stg + L.b_hi + re0, hr[0], hr[1], hr[2], hr[3]);
+          st_shared_v4(stg + L.b_hi + re1, hr[4], hr[5], hr[6], hr[7]);
+          st_shared_v4(stg + L.b_lo + re0, lr[0], lr[1], lr[2], lr[3]);
+          st_shared_v4(stg + L.b_lo + re1, lr[4], lr[5], lr[6], lr[7]);
+          st_shared_v4(stg + L.b_hi + im0, hm[0], hm[1], hm[2], hm[3]);
+          st_shared_v4(stg + L.b_hi + im1, hm[4], hm[5], hm[6], hm[7]);
+          st_shared_v4(stg + L.b_lo + im0, lm[0], lm[1], lm[2], lm[3]);
+          st_shared_v4(stg + L.b_lo + im1, lm[4], lm[5], lm[6], lm[7]);
+        }
+        // next stage's phase table into the other parity buffer: its last
+        // readers (stage st - 1) are past this stage's barrier
+        if (st + 1 < U.n_stages) {
+          const int st1 = st + 1;
+          const double *pb = pos_all + ((st1 / kTcStagesPerBlock) & 1) * 3 * kTcBlockNodes +
+                             (st1 & (kTcStagesPerBlock - 1)) * kTcNodes;
+          float2 *et = etab + (st1 & 1) * Qt * kEStride;
+          if (t_on0) tc_phase_pair(pb, et, tq, tn, kx0, ky0, kz0);
+          if (t_on1) tc_phase_pair(pb, et, tq + 32, tn, kx1, ky1, kz1);
         }
       }
-      while (next_drain < U.n_groups) {
-        tc_drain(p, U, accfull, accfree, tmem, gbase + next_drain, next_drain == 0, next_drain == U.n_groups - 1,
-                 abort_flag);
+      ptx::fence_proxy_async_smem();
+      // drain the previous group a few stages into the current one, when the
+      // MMAs that wrote it have (almost surely) completed
+      if (st % kTcDrain == kTcStages - 1 && st / kTcDrain >= 1 && next_drain == st / kTcDrain - 1) {
+        tc_drain(p, W, U, accfull, tmem, gbase + next_drain, next_drain == 0, false, abort_flag);
         ++next_drain;
       }
-      if (U.n_groups == 0 && tid < kTcRows && row < U.P_tile) {
-        // no nodes in this split: its share of the tile is zero
-        float2 *dst = p.out + (int64_t)U.split * p.S * p.V;
-        const int s_row = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz + U.it.q0 : U.it.p0 + row);
-        for (int q = 0; q < U.Q_tile; ++q)
-          for (int v = 0; v < p.VG; ++v) dst[(int64_t)(s_row + q) * p.V + p.v0 + v] = make_float2(0.f, 0.f);
-      }
-      gbase += U.n_groups;
     }
-  } else if (tid == kTcMmaWarp * 32) {
-    // ------------------------------------------------------ MMA issue --
-    int gst = 0, gbase = 0;
-    for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
-      const TcUnit U = tc_unit(p, u);
-      for (int st = 0; st < U.n_stages; ++st, ++gst) {
-        const int s = gst % kTcStages;
-        const uint32_t round = gst / kTcStages;
-        const int gg = gbase + st / kTcDrain;
-        const int b = gg & 1;
-        const bool group_start = (st % kTcDrain) == 0;
-        if (group_start && gg >= 2) tc_wait(&accfree[b], ((gg - 2) >> 1) & 1, abort_flag);
-        tc_wait(&full[s], round & 1, abort_flag);
-        ptx::tc_fence_after();
-        const uint32_t stage = sbase + s * L.stage_bytes;
-        const uint32_t acc = tmem + (uint32_t)(b * p.acc_cols);
-#pragma unroll
-        for (int ks = 0; ks < 2; ++ks) {
-          const uint64_t ah = ptx::smem_desc(stage + L.a_hi + ks * kTcRows * 32, 128, 256);
-          const uint64_t al = ptx::smem_desc(stage + L.a_lo + ks * kTcRows * 32, 128, 256);
-          const uint64_t bh = ptx::smem_desc(stage + L.b_hi + ks * p.NT * 32, 128, 256);
-          const uint64_t bl = ptx::smem_desc(stage + L.b_lo + ks * p.NT * 32, 128, 256);
-          ptx::mma_bf16(acc, ah, bh, idesc, (group_start && ks == 0) ? 0u : 1u);
-          ptx::mma_bf16(acc, ah, bl, idesc, 1u);
-          ptx::mma_bf16(acc, al, bh, idesc, 1u);
-        }
-        ptx::mma_commit(&empty[s]);
-        if ((st % kTcDrain) == kTcDrain - 1 || st == U.n_stages - 1) ptx::mma_commit(&accfull[b]);
-      }
-      gbase += U.n_groups;
+    if (U.n_stages > 0) {
+      ptx::named_barrier(1, kTcProducers);  // the unit's last stage is written
+      if (issuer)
+        tc_issue(L, sbase, tmem, idesc, NT, p.acc_cols, empty, accfull, gst - 1, U.n_stages - 1, U.n_stages,
+                 gbase + (U.n_stages - 1) / kTcDrain);
     }
+    while (next_drain < U.n_groups) {
+      tc_drain(p, W, U, accfull, tmem, gbase + next_drain, next_drain == 0, next_drain == U.n_groups - 1,
+               abort_flag);
+      ++next_drain;
+    }
+    if (U.n_groups == 0 && tid < kTcRows && tid < U.P_tile) {
+      // no nodes in this split: its share of the tile is zero
+      float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
+      const int s_row = U.run.start + (fac ? (U.it.p0 + tid) * p.n_kz + U.it.q0 : U.it.p0 + tid);
+      for (int q = 0; q < U.Q_tile; ++q)
+        for (int v = 0; v < VG; ++v) dst[(int64_t)(s_row + q) * p.V + p.v0 + v] = make_float2(0.f, 0.f);
+    }
+    gbase += U.n_groups;
+  }
+  if (issuer) {
     // all issued MMAs complete before the tensor memory is released
     ptx::mma_commit(done);
     if (!ptx::mbar_wait(done, 0, kTcWaitNs)) *abort_flag = 1;
@@ -515,7 +604,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(TcDev p_in, in
   ptx::tc_fence_before();
   __syncthreads();
   if (tid == 0 && *abort_flag) atomicOr(p.error, kErrTimeout);
-  if (warp == kTcMmaWarp) {
+  if (warp == 0) {
     ptx::tc_fence_after();
     ptx::tmem_dealloc(tmem, 2 * p.acc_cols);
   }
