@@ -30,7 +30,6 @@
 // running sum.  Blocks loop over work units (row/column tile of a run x node
 // range).  All waits are bounded: on timeout the block records an error,
 // lets its MMAs finish and frees its tensor memory.
-#include <cuda_bf16.h>
 #include <cmath>
 #include <cub/cub.cuh>
 
@@ -144,15 +143,16 @@ __host__ __device__ inline uint32_t kmajor_offset(uint32_t row, uint32_t k, uint
   return (k >> 4) * (rows * 32) + (row >> 3) * 256 + ((k >> 3) & 1) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
-__device__ inline uint32_t bf16x2_bits(__nv_bfloat162 h) { return *reinterpret_cast<uint32_t *>(&h); }
-
 // hi = bf16(x), lo = bf16(x - hi) for the pair (a, b); bits of (hi_a, hi_b)
-// and (lo_a, lo_b) with a in the low half.
+// and (lo_a, lo_b) with a in the low half (cvt.rn.bf16x2 puts its first
+// source in the upper half).
 __device__ inline void split_pair(float a, float b, uint32_t &hi, uint32_t &lo) {
-  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-  const float2 hf = __bfloat1622float2(h);
-  hi = bf16x2_bits(h);
-  lo = bf16x2_bits(__floats2bfloat162_rn(a - hf.x, b - hf.y));
+  uint32_t h, l;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(h) : "f"(b), "f"(a));
+  const float ha = __uint_as_float(h << 16), hb = __uint_as_float(h & 0xffff0000u);
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(l) : "f"(b - hb), "f"(a - ha));
+  hi = h;
+  lo = l;
 }
 
 // cos and sin of 2 pi c for c in cycles given in FP64: c is reduced modulo
@@ -341,9 +341,9 @@ __device__ inline void tc_drain(const TcDev &p, const TcWork &W, const TcUnit &U
 // empty[s], and the group's accumulator by a commit to accfull[gg & 1] after
 // its last stage.
 __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, uint32_t idesc, int NT,
-                                int acc_cols, uint64_t *empty, uint64_t *accfull, int g, int st, int n_stages,
+                                int acc_cols, uint64_t *empty, uint64_t *accfull, uint32_t g, uint32_t st, uint32_t n_stages,
                                 int gg) {
-  const int s = g % kTcStages;
+  const uint32_t s = g % kTcStages;
   const int b = gg & 1;
   const bool group_start = (st % kTcDrain) == 0;
   ptx::tc_fence_after();
@@ -402,30 +402,45 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   // 32 ((w - 8) >> 1) + lane, same node halves, and the next stage's phase
   // table.  Threads 0-127 also derive the node blocks.  One thread of warp 7
   // issues a stage's MMAs after the block barrier that follows the stage
-  // (every writer has fenced its stores to the async proxy by then).
+  // (every writer has fenced its stores to the async proxy by then).  Both
+  // roles pass the same barriers and drains in the same order.
   const bool a_role = warp < 8;
   const int rw = a_role ? warp : warp - 8;
   const int row = (rw >> 1) * 32 + lane;  // A row or B pair
   const int half = rw & 1;                // nodes 8 half .. 8 half + 7 of a stage
   const bool loader = tid < kTcBlockNodes;
   const bool issuer = tid == 7 * 32;
-  // operand addresses inside a stage (K chunk 2 half and 2 half + 1 of 8)
-  const uint32_t a0 = kmajor_offset(row, 16 * half, kTcRows), a1 = kmajor_offset(row, 16 * half + 8, kTcRows);
+  // operand addresses inside a stage (K chunks 2 half and 2 half + 1 of 8)
+  uint32_t o_hi0, o_hi1, o_lo0, o_lo1, o_ih0 = 0, o_ih1 = 0, o_il0 = 0, o_il1 = 0;
+  if (a_role) {
+    o_hi0 = L.a_hi + kmajor_offset(row, 16 * half, kTcRows);
+    o_hi1 = L.a_hi + kmajor_offset(row, 16 * half + 8, kTcRows);
+    o_lo0 = L.a_lo + kmajor_offset(row, 16 * half, kTcRows);
+    o_lo1 = L.a_lo + kmajor_offset(row, 16 * half + 8, kTcRows);
+  } else {
+    o_hi0 = L.b_hi + kmajor_offset(row, 16 * half, NT);
+    o_hi1 = L.b_hi + kmajor_offset(row, 16 * half + 8, NT);
+    o_lo0 = L.b_lo + kmajor_offset(row, 16 * half, NT);
+    o_lo1 = L.b_lo + kmajor_offset(row, 16 * half + 8, NT);
+    o_ih0 = L.b_hi + kmajor_offset(NH + row, 16 * half, NT);
+    o_ih1 = L.b_hi + kmajor_offset(NH + row, 16 * half + 8, NT);
+    o_il0 = L.b_lo + kmajor_offset(NH + row, 16 * half, NT);
+    o_il1 = L.b_lo + kmajor_offset(NH + row, 16 * half + 8, NT);
+  }
   const bool b_rows = row < NH;
-  const uint32_t re0 = kmajor_offset(row, 16 * half, NT), re1 = kmajor_offset(row, 16 * half + 8, NT);
-  const uint32_t im0 = kmajor_offset(NH + row, 16 * half, NT), im1 = kmajor_offset(NH + row, 16 * half + 8, NT);
   // phase-table thread: q = (tid - 256) / 8 (+ 32), nodes 2 ((tid - 256) % 8) + {0, 1}
   const int tq = (tid - 256) >> 3, tn = ((tid - 256) & 7) * 2;
-  int gst = 0, gbase = 0;
+  uint32_t gst = 0;
+  int gbase = 0;
   TcRaw raw;
   for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
     const TcUnit U = tc_unit(p, W, u);
     const bool fac = U.run.factored != 0;
+    const uint32_t nst = (uint32_t)U.n_stages;
     ptx::named_barrier(1, kTcProducers);  // the previous unit's readers are done
     // per-unit row data in registers
     double kx0 = 0, ky0 = 0, kz0 = 0, kx1 = 0, ky1 = 0, kz1 = 0;  // A: kp of the row; B: kq of q and q + 32
     int bq = 0, bv = 0;
-    const bool a_warp_active = a_role && (rw >> 1) * 32 < U.P_tile;
     if (a_role) {
       if (row < U.P_tile) {
         const int s_p = U.run.start + (fac ? (U.it.p0 + row) * p.n_kz : U.it.p0 + row);
@@ -457,71 +472,87 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     const bool t_on0 = !a_role && fac && tq < U.Q_tile, t_on1 = !a_role && fac && tq + 32 < U.Q_tile;
     const float *wrun = p.weights ? p.weights + (int64_t)U.it.run * p.md.slots : nullptr;
     const float tg = (float)p.run_t[U.it.run];
-    const int n_blocks = (int)ceil_div(U.n_stages, kTcStagesPerBlock);
+    const uint32_t n_blocks = (nst + kTcStagesPerBlock - 1) / kTcStagesPerBlock;
     // prologue: node block 0 into buffer 0
-    if (loader && U.n_stages > 0) {
+    if (loader && nst > 0) {
       const int64_t n = U.n_begin + tid;
       if (n < U.n_end) tc_load_raw(p, n, raw);
       tc_derive(p, U, n, raw, wrun, tg, pos_all, w_all, tid);
     }
     ptx::named_barrier(1, kTcProducers);  // block 0 is visible
-    if (U.n_stages > 0) {
+    if (nst > 0) {
       if (t_on0) tc_phase_pair(pos_all, etab, tq, tn, kx0, ky0, kz0);
       if (t_on1) tc_phase_pair(pos_all, etab, tq + 32, tn, kx1, ky1, kz1);
     }
+    const uint32_t g0 = gst;
     int next_drain = 0;
-
-    for (int st = 0; st < U.n_stages; ++st, ++gst) {
-      const int s = gst & (kTcStages - 1);
-      const uint32_t round = (uint32_t)gst / kTcStages;
-      const int j = st & (kTcStagesPerBlock - 1);
-      const int blk = st / kTcStagesPerBlock;
-      const int buf = blk & 1;
-      if (loader && blk + 1 < n_blocks) {
-        // block blk + 1 (block blk is then complete): raw loads issued at
-        // j == 4, derived into the other buffer at j == 6.  That buffer's
-        // readers (stages of block blk - 1) passed this block's first barrier.
-        const int64_t n1 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes + tid;
-        if (j == 4 && n1 < U.n_end) tc_load_raw(p, n1, raw);
-        if (j == 6)
-          tc_derive(p, U, n1, raw, wrun, tg, pos_all + (buf ^ 1) * 3 * kTcBlockNodes,
-                    w_all + (buf ^ 1) * VG * kWStride, tid);
-      }
-      // wait until the MMAs that last read stage s are done
-      tc_wait(&empty[s], (round & 1) ^ 1, abort_flag);
-      // every writer of the previous stage is done (its MMAs go out now); the
-      // phase table of this stage and the node blocks derived up to the
-      // previous stage are visible
-      ptx::named_barrier(1, kTcProducers);
-      if (issuer && st > 0)
-        tc_issue(L, sbase, tmem, idesc, NT, p.acc_cols, empty, accfull, gst - 1, st - 1, U.n_stages,
-                 gbase + (st - 1) / kTcDrain);
-      const uint32_t stg = sbase + s * L.stage_bytes;
-      const int nb = j * kTcNodes + 8 * half;  // first node of this thread in the block
-      if (a_warp_active) {
-        // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n
-        const double *px = pos_all + buf * 3 * kTcBlockNodes + nb;
-        uint32_t h[8], l[8];
-#pragma unroll
-        for (int u4 = 0; u4 < 8; u4 += 2) {
-          const double2 x = *reinterpret_cast<const double2 *>(px + u4);
-          const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
-          const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
-          float c0, s0, c1, s1;
-          cycles_cos_sin(fma(kz0, z.x, fma(ky0, y.x, kx0 * x.x)), c0, s0);
-          cycles_cos_sin(fma(kz0, z.y, fma(ky0, y.y, kx0 * x.y)), c1, s1);
-          split_pair(c0, s0, h[u4], l[u4]);
-          split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
+    if (a_role) {
+      // ------------------------------------------------------- A rows --
+      const bool active = (rw >> 1) * 32 < U.P_tile;
+      for (uint32_t st = 0; st < nst; ++st) {
+        const uint32_t g = g0 + st, s = g & (kTcStages - 1);
+        const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
+        if (loader && blk + 1 < n_blocks && (j == 4 || j == 6)) {
+          // block blk + 1 (block blk is then complete): raw loads issued at
+          // j == 4, derived into the other buffer at j == 6.  That buffer's
+          // readers (stages of block blk - 1) passed this block's first barrier.
+          const int64_t n1 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes + tid;
+          if (j == 4) {
+            if (n1 < U.n_end) tc_load_raw(p, n1, raw);
+          } else {
+            tc_derive(p, U, n1, raw, wrun, tg, pos_all + (buf ^ 1) * 3 * kTcBlockNodes,
+                      w_all + (buf ^ 1) * VG * kWStride, tid);
+          }
         }
-        st_shared_v4(stg + L.a_hi + a0, h[0], h[1], h[2], h[3]);
-        st_shared_v4(stg + L.a_hi + a1, h[4], h[5], h[6], h[7]);
-        st_shared_v4(stg + L.a_lo + a0, l[0], l[1], l[2], l[3]);
-        st_shared_v4(stg + L.a_lo + a1, l[4], l[5], l[6], l[7]);
-      } else if (!a_role) {
+        // wait until the MMAs that last read stage s are done
+        tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
+        // every writer of the previous stage is done (its MMAs go out now); the
+        // phase table of this stage and the node blocks derived up to the
+        // previous stage are visible
+        ptx::named_barrier(1, kTcProducers);
+        if (issuer && st > 0)
+          tc_issue(L, sbase, tmem, idesc, NT, p.acc_cols, empty, accfull, g - 1, st - 1, nst,
+                   gbase + (st - 1) / kTcDrain);
+        if (active) {
+          // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n
+          const uint32_t stg = sbase + s * L.stage_bytes;
+          const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 8 * half;
+          uint32_t h[8], l[8];
+#pragma unroll
+          for (int u4 = 0; u4 < 8; u4 += 2) {
+            const double2 x = *reinterpret_cast<const double2 *>(px + u4);
+            const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
+            const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
+            float c0, s0, c1, s1;
+            cycles_cos_sin(fma(kz0, z.x, fma(ky0, y.x, kx0 * x.x)), c0, s0);
+            cycles_cos_sin(fma(kz0, z.y, fma(ky0, y.y, kx0 * x.y)), c1, s1);
+            split_pair(c0, s0, h[u4], l[u4]);
+            split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
+          }
+          st_shared_v4(stg + o_hi0, h[0], h[1], h[2], h[3]);
+          st_shared_v4(stg + o_hi1, h[4], h[5], h[6], h[7]);
+          st_shared_v4(stg + o_lo0, l[0], l[1], l[2], l[3]);
+          st_shared_v4(stg + o_lo1, l[4], l[5], l[6], l[7]);
+        }
+        ptx::fence_proxy_async_smem();
+        // drain the previous group a few stages into the current one, when the
+        // MMAs that wrote it have (almost surely) completed
+        if ((st & (kTcDrain - 1)) == kTcStages - 1 && st >= kTcDrain) {
+          tc_drain(p, W, U, accfull, tmem, gbase + next_drain, next_drain == 0, false, abort_flag);
+          ++next_drain;
+        }
+      }
+    } else {
+      // ------------------------------------------------------- B rows --
+      for (uint32_t st = 0; st < nst; ++st) {
+        const uint32_t g = g0 + st, s = g & (kTcStages - 1);
+        const uint32_t j = st & (kTcStagesPerBlock - 1), buf = (st / kTcStagesPerBlock) & 1;
+        tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
+        ptx::named_barrier(1, kTcProducers);
         // B'^T rows: re row `row` = (Re B, Im B), im row NT/2 + row =
         // (Im B, -Re B), B = e_q(n) W'(n, v).  Pairs past Q_tile VG hold
         // values no output reads.
-        const float4 *wp = reinterpret_cast<const float4 *>(w_all + (buf * VG + bv) * kWStride + nb);
+        const float4 *wp = reinterpret_cast<const float4 *>(w_all + (buf * VG + bv) * kWStride + j * kTcNodes + 8 * half);
         float br[8], bi[8];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -529,7 +560,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           br[2 * i] = w2.x; bi[2 * i] = w2.y; br[2 * i + 1] = w2.z; bi[2 * i + 1] = w2.w;
         }
         if (fac) {
-          const float4 *ep = reinterpret_cast<const float4 *>(etab + ((st & 1) * Qt + bq) * kEStride + nb - j * kTcNodes);
+          const float4 *ep = reinterpret_cast<const float4 *>(etab + ((st & 1) * Qt + bq) * kEStride + 8 * half);
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const float4 e2 = ep[i];
@@ -548,39 +579,39 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           lm[i] = __byte_perm(lr[i], 0u, 0x1032) ^ 0x80000000u;
         }
         if (b_rows) {
-          st_shared_v4(stg + L.b_hi + re0, hr[0], hr[1], hr[2], hr[3]);
-          st_shared_v4(stg + L.b_hi + re1, hr[4], hr[5], hr[6], hr[7]);
-          st_shared_v4(stg + L.b_lo + re0, lr[0], lr[1], lr[2], lr[3]);
-          st_shared_v4(stg + L.b_lo + re1, lr[4], lr[5], lr[6], lr[7]);
-          st_shared_v4(stg + L.b_hi + im0, hm[0], hm[1], hm[2], hm[3]);
-          st_shared_v4(stg + L.b_hi + im1, hm[4], hm[5], hm[6], hm[7]);
-          st_shared_v4(stg + L.b_lo + im0, lm[0], lm[1], lm[2], lm[3]);
-          st_shared_v4(stg + L.b_lo + im1, lm[4], lm[5], lm[6], lm[7]);
+          const uint32_t stg = sbase + s * L.stage_bytes;
+          st_shared_v4(stg + o_hi0, hr[0], hr[1], hr[2], hr[3]);
+          st_shared_v4(stg + o_hi1, hr[4], hr[5], hr[6], hr[7]);
+          st_shared_v4(stg + o_lo0, lr[0], lr[1], lr[2], lr[3]);
+          st_shared_v4(stg + o_lo1, lr[4], lr[5], lr[6], lr[7]);
+          st_shared_v4(stg + o_ih0, hm[0], hm[1], hm[2], hm[3]);
+          st_shared_v4(stg + o_ih1, hm[4], hm[5], hm[6], hm[7]);
+          st_shared_v4(stg + o_il0, lm[0], lm[1], lm[2], lm[3]);
+          st_shared_v4(stg + o_il1, lm[4], lm[5], lm[6], lm[7]);
         }
         // next stage's phase table into the other parity buffer: its last
         // readers (stage st - 1) are past this stage's barrier
-        if (st + 1 < U.n_stages) {
-          const int st1 = st + 1;
+        if (t_on0 && st + 1 < nst) {
+          const uint32_t st1 = st + 1;
           const double *pb = pos_all + ((st1 / kTcStagesPerBlock) & 1) * 3 * kTcBlockNodes +
                              (st1 & (kTcStagesPerBlock - 1)) * kTcNodes;
           float2 *et = etab + (st1 & 1) * Qt * kEStride;
-          if (t_on0) tc_phase_pair(pb, et, tq, tn, kx0, ky0, kz0);
+          tc_phase_pair(pb, et, tq, tn, kx0, ky0, kz0);
           if (t_on1) tc_phase_pair(pb, et, tq + 32, tn, kx1, ky1, kz1);
         }
-      }
-      ptx::fence_proxy_async_smem();
-      // drain the previous group a few stages into the current one, when the
-      // MMAs that wrote it have (almost surely) completed
-      if (st % kTcDrain == kTcStages - 1 && st / kTcDrain >= 1 && next_drain == st / kTcDrain - 1) {
-        tc_drain(p, W, U, accfull, tmem, gbase + next_drain, next_drain == 0, false, abort_flag);
-        ++next_drain;
+        ptx::fence_proxy_async_smem();
+        if ((st & (kTcDrain - 1)) == kTcStages - 1 && st >= kTcDrain) {
+          tc_drain(p, W, U, accfull, tmem, gbase + next_drain, next_drain == 0, false, abort_flag);
+          ++next_drain;
+        }
       }
     }
-    if (U.n_stages > 0) {
+    gst = g0 + nst;
+    if (nst > 0) {
       ptx::named_barrier(1, kTcProducers);  // the unit's last stage is written
       if (issuer)
-        tc_issue(L, sbase, tmem, idesc, NT, p.acc_cols, empty, accfull, gst - 1, U.n_stages - 1, U.n_stages,
-                 gbase + (U.n_stages - 1) / kTcDrain);
+        tc_issue(L, sbase, tmem, idesc, NT, p.acc_cols, empty, accfull, gst - 1, nst - 1, nst,
+                 gbase + (nst - 1) / kTcDrain);
     }
     while (next_drain < U.n_groups) {
       tc_drain(p, W, U, accfull, tmem, gbase + next_drain, next_drain == 0, next_drain == U.n_groups - 1,
