@@ -48,10 +48,11 @@ constexpr int kTcProducers = 32 * kTcProducerWarps;  // every thread of the bloc
 constexpr int kTcThreads = kTcProducers;
 constexpr int kTcIssuer = 96;       // thread that issues the MMAs (warp 3: A rows 96-127)
 constexpr int kTcVGroup = 8;        // Mxy columns per launch
-// Stages accumulated in one tensor-memory accumulator before it is drained
-// into an FP32 round-to-nearest running sum.  The tensor core's FP32
-// accumulation truncates, so its error grows with the number of MMAs added
-// into one accumulator; 32 stages (512 nodes, 192 MMAs) keep it near 1e-5.
+// Stages accumulated in the tensor-memory accumulator before it is folded
+// into an FP32 round-to-nearest running sum (also in tensor memory).  The
+// tensor core's FP32 accumulation truncates, so its error grows with the
+// number of MMAs added into one accumulator; 32 stages (512 nodes, 192 MMAs)
+// keep it near 1e-5.
 constexpr int kTcDrain = 32;
 constexpr uint64_t kTcWaitNs = 2000000000ull;
 constexpr uint32_t kAStageBytes = kTcRows * 2 * kTcNodes * 2;  // 128 rows x 32 K x bf16 = 8 KB
@@ -80,7 +81,6 @@ struct TcDev {
   const int *plan;  // device: [2] factored items, [3] generic items, [4] splits, [5] nodes per split
   float2 *partials; // (splits, S, V) when splits > 1
   float2 *out;
-  float *scratch;  // per block: 128 x NT running sums
   int *error;
 };
 
@@ -276,79 +276,99 @@ __device__ inline void tc_phase_pair(const double *pb, float2 *et, int q, int n0
   *reinterpret_cast<float4 *>(et + q * kEStride + n0) = make_float4(c0, -s0, c1, -s1);
 }
 
-// Adds accumulator `b` (one drained group) into the block's running sums,
-// or, for the unit's last group, writes running sums + accumulator to the
-// output samples.  Accumulator columns: pair j's real part in column j, its
-// imaginary part in column NT/2 + j.  Warp w reads TMEM lanes of quarter
-// w % 4 and every fourth chunk of 8 pairs starting at w / 4.
-__device__ inline void tc_drain(const TcDev &p, const TcWork &W, const TcUnit &U, uint64_t *accfull, uint32_t tmem,
-                                int gg, bool first, bool final, volatile int *abort_flag) {
+// Tensor memory: the accumulator in columns [0, NT) and the FP32 running sum
+// in [acc_cols, acc_cols + NT).  Accumulator column j < NT/2 is the real
+// part of pair j, column NT/2 + j its imaginary part.
+
+// Folds the accumulator (group gg, complete once accfull's phase gg & 1
+// has flipped) into the running sum: sum = acc (first group) or sum + acc,
+// in FP32 round-to-nearest.  Warp w handles TMEM lanes of quarter w % 4 and
+// column quarter w / 4.  The next MMA into the accumulator is issued after a
+// block barrier.
+__device__ inline void tc_fold(const TcDev &p, uint64_t *accfull, uint32_t tmem, int gg, bool first,
+                               volatile int *abort_flag) {
+  const int warp = threadIdx.x >> 5;
+  tc_wait(accfull, gg & 1, abort_flag);
+  ptx::tc_fence_after();
+  const int quarter = warp & 3, cq = warp >> 2;
+  const int cpq = ((p.NT / 4 + 15) / 16) * 16;
+  const int c_begin = cq * cpq, c_end = min(p.NT, c_begin + cpq);
+  const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
+  for (int c0 = c_begin; c0 < c_end; c0 += 16) {
+    uint32_t a[16];
+    ptx::tmem_ld16(tmem + lanes + (uint32_t)c0, a);
+    if (!first) {
+      // the running sum in two halves of 8 columns (fewer live registers)
+      uint32_t r[8];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        ptx::tmem_ld8(tmem + lanes + (uint32_t)(p.acc_cols + c0 + 8 * h), r);
+        ptx::tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          a[8 * h + i] = __float_as_uint(__uint_as_float(r[i]) + __uint_as_float(a[8 * h + i]));
+      }
+    } else {
+      ptx::tmem_wait_ld();
+    }
+    ptx::tmem_st16(tmem + lanes + (uint32_t)(p.acc_cols + c0), a);
+  }
+  ptx::tmem_wait_st();
+  ptx::tc_fence_before();
+}
+
+// Writes the unit's result: running sum (when earlier groups were folded) +
+// accumulator of the last group gg, to the output samples.  Warp w reads TMEM
+// lanes of quarter w % 4 and every fourth chunk of 8 pairs starting at w / 4.
+__device__ inline void tc_final(const TcDev &p, const TcWork &W, const TcUnit &U, uint64_t *accfull, uint32_t tmem,
+                                int gg, bool has_sum, volatile int *abort_flag) {
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int b = gg & 1;
-  tc_wait(&accfull[b], (gg >> 1) & 1, abort_flag);
+  tc_wait(accfull, gg & 1, abort_flag);
   ptx::tc_fence_after();
   const int quarter = warp & 3;
   const int row = quarter * 32 + (tid & 31);
   const int NH = p.NT >> 1;
-  float *srow = p.scratch + ((size_t)blockIdx.x * kTcRows + row) * p.NT;
   const bool row_ok = row < U.P_tile;
   float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
   const int s_row = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz + U.it.q0 : U.it.p0 + row);
-  const uint32_t taddr = tmem + (uint32_t)(b * p.acc_cols) + ((uint32_t)(quarter * 32) << 16);
+  const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
   for (int c0 = (warp >> 2) * 8; c0 < NH; c0 += 32) {
-    // running sums first, so their loads overlap the tensor-memory reads
-    float4 re0 = make_float4(0.f, 0.f, 0.f, 0.f), re1 = re0, im0 = re0, im1 = re0;
-    if (!first && row_ok) {
-      re0 = *reinterpret_cast<const float4 *>(srow + c0);
-      re1 = *reinterpret_cast<const float4 *>(srow + c0 + 4);
-      im0 = *reinterpret_cast<const float4 *>(srow + NH + c0);
-      im1 = *reinterpret_cast<const float4 *>(srow + NH + c0 + 4);
-    }
-    uint32_t r[8], m[8];
+    uint32_t r[8], m[8], sr[8], sm[8];
     ptx::tmem_ld8(taddr + (uint32_t)c0, r);
     ptx::tmem_ld8(taddr + (uint32_t)(NH + c0), m);
+    if (has_sum) {
+      ptx::tmem_ld8(taddr + (uint32_t)(p.acc_cols + c0), sr);
+      ptx::tmem_ld8(taddr + (uint32_t)(p.acc_cols + NH + c0), sm);
+    }
     ptx::tmem_wait_ld();
     if (!row_ok) continue;
-    re0.x += __uint_as_float(r[0]); re0.y += __uint_as_float(r[1]); re0.z += __uint_as_float(r[2]);
-    re0.w += __uint_as_float(r[3]); re1.x += __uint_as_float(r[4]); re1.y += __uint_as_float(r[5]);
-    re1.z += __uint_as_float(r[6]); re1.w += __uint_as_float(r[7]);
-    im0.x += __uint_as_float(m[0]); im0.y += __uint_as_float(m[1]); im0.z += __uint_as_float(m[2]);
-    im0.w += __uint_as_float(m[3]); im1.x += __uint_as_float(m[4]); im1.y += __uint_as_float(m[5]);
-    im1.z += __uint_as_float(m[6]); im1.w += __uint_as_float(m[7]);
-    if (!final) {
-      *reinterpret_cast<float4 *>(srow + c0) = re0;
-      *reinterpret_cast<float4 *>(srow + c0 + 4) = re1;
-      *reinterpret_cast<float4 *>(srow + NH + c0) = im0;
-      *reinterpret_cast<float4 *>(srow + NH + c0 + 4) = im1;
-    } else {
-      const float rv[8] = {re0.x, re0.y, re0.z, re0.w, re1.x, re1.y, re1.z, re1.w};
-      const float iv[8] = {im0.x, im0.y, im0.z, im0.w, im1.x, im1.y, im1.z, im1.w};
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int jj = c0 + i;  // pair (q, v)
-        const int q = jj / p.VG, vv = jj % p.VG;
-        if (q < U.Q_tile) dst[(int64_t)(s_row + q) * p.V + p.v0 + vv] = make_float2(rv[i], iv[i]);
+    for (int i = 0; i < 8; ++i) {
+      float re = __uint_as_float(r[i]), im = __uint_as_float(m[i]);
+      if (has_sum) {
+        re = __uint_as_float(sr[i]) + re;
+        im = __uint_as_float(sm[i]) + im;
       }
+      const int jj = c0 + i;  // pair (q, v)
+      const int q = jj / p.VG, vv = jj % p.VG;
+      if (q < U.Q_tile) dst[(int64_t)(s_row + q) * p.V + p.v0 + vv] = make_float2(re, im);
     }
   }
-  // the next MMA into this accumulator is issued after a block barrier
   ptx::tc_fence_before();
 }
 
 // MMAs of one stage (global stage index g, stage-local st of a unit with
-// n_stages stages, accumulator group gg): A_hi B_hi + A_hi B_lo + A_lo B_hi
-// over the two K steps; the stage's shared memory is released by a commit to
-// empty[s], and the group's accumulator by a commit to accfull[gg & 1] after
-// its last stage.
+// n_stages stages): A_hi B_hi + A_hi B_lo + A_lo B_hi over the two K steps
+// into the accumulator (overwritten at a group's first stage); the stage's
+// shared memory is released by a commit to empty[s], and the group's
+// accumulator by a commit to accfull after the group's last stage.
 __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, uint32_t idesc, int NT,
-                                int acc_cols, uint64_t *empty, uint64_t *accfull, uint32_t g, uint32_t st, uint32_t n_stages,
-                                int gg) {
+                                uint64_t *empty, uint64_t *accfull, uint32_t g, uint32_t st, uint32_t n_stages) {
   const uint32_t s = g % kTcStages;
-  const int b = gg & 1;
   const bool group_start = (st % kTcDrain) == 0;
   ptx::tc_fence_after();
   const uint32_t stage = sbase + s * L.stage_bytes;
-  const uint32_t acc = tmem + (uint32_t)(b * acc_cols);
+  const uint32_t acc = tmem;
 #pragma unroll
   for (int ks = 0; ks < 2; ++ks) {
     const uint64_t ah = ptx::smem_desc(stage + L.a_hi + ks * kTcRows * 32, 128, 256);
@@ -360,7 +380,7 @@ __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, 
     ptx::mma_bf16(acc, al, bh, idesc, 1u);
   }
   ptx::mma_commit(&empty[s]);
-  if ((st % kTcDrain) == kTcDrain - 1 || st == n_stages - 1) ptx::mma_commit(&accfull[b]);
+  if ((st % kTcDrain) == kTcDrain - 1 || st == n_stages - 1) ptx::mma_commit(accfull);
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_constant__ TcDev p, int kind) {
@@ -375,7 +395,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   const TcSmem L = tc_smem_layout(NT, VG, Qt);
   uint64_t *empty = reinterpret_cast<uint64_t *>(smem + L.bars);
   uint64_t *accfull = empty + kTcStages;
-  uint64_t *done = accfull + 2;
+  uint64_t *done = accfull + 1;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L.misc);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + L.misc + 4);
   double *pos_all = reinterpret_cast<double *>(smem + L.pos);
@@ -385,7 +405,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
 
   if (tid == 0) {
     for (int s = 0; s < kTcStages; ++s) ptx::mbar_init(&empty[s], 1);
-    for (int b = 0; b < 2; ++b) ptx::mbar_init(&accfull[b], 1);
+    ptx::mbar_init(accfull, 1);
     ptx::mbar_init(done, 1);
     *abort_flag = 0;
     ptx::fence_mbar_init();
@@ -511,8 +531,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         // previous stage are visible
         ptx::named_barrier(1, kTcProducers);
         if (issuer && st > 0)
-          tc_issue(L, sbase, tmem, idesc, NT, p.acc_cols, empty, accfull, g - 1, st - 1, nst,
-                   gbase + (st - 1) / kTcDrain);
+          tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g - 1, st - 1, nst);
         if (active) {
           // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n
           const uint32_t stg = sbase + s * L.stage_bytes;
@@ -535,10 +554,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           st_shared_v4(stg + o_lo1, l[4], l[5], l[6], l[7]);
         }
         ptx::fence_proxy_async_smem();
-        // drain the previous group a few stages into the current one, when the
-        // MMAs that wrote it have (almost surely) completed
-        if ((st & (kTcDrain - 1)) == kTcStages - 1 && st >= kTcDrain) {
-          tc_drain(p, W, U, accfull, tmem, gbase + next_drain, next_drain == 0, false, abort_flag);
+        // the previous group's last MMAs went out at this stage's barrier:
+        // fold the accumulator into the running sum before the next group
+        // starts (its first MMAs go out at the next stage's barrier)
+        if ((st & (kTcDrain - 1)) == 0 && st > 0) {
+          tc_fold(p, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
       }
@@ -600,8 +620,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           if (t_on1) tc_phase_pair(pb, et, tq + 32, tn, kx1, ky1, kz1);
         }
         ptx::fence_proxy_async_smem();
-        if ((st & (kTcDrain - 1)) == kTcStages - 1 && st >= kTcDrain) {
-          tc_drain(p, W, U, accfull, tmem, gbase + next_drain, next_drain == 0, false, abort_flag);
+        if ((st & (kTcDrain - 1)) == 0 && st > 0) {
+          tc_fold(p, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
       }
@@ -610,14 +630,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     if (nst > 0) {
       ptx::named_barrier(1, kTcProducers);  // the unit's last stage is written
       if (issuer)
-        tc_issue(L, sbase, tmem, idesc, NT, p.acc_cols, empty, accfull, gst - 1, nst - 1, nst,
-                 gbase + (nst - 1) / kTcDrain);
+        tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, gst - 1, nst - 1, nst);
     }
-    while (next_drain < U.n_groups) {
-      tc_drain(p, W, U, accfull, tmem, gbase + next_drain, next_drain == 0, next_drain == U.n_groups - 1,
-               abort_flag);
-      ++next_drain;
-    }
+    if (U.n_groups > 0) tc_final(p, W, U, accfull, tmem, gbase + U.n_groups - 1, U.n_groups > 1, abort_flag);
     if (U.n_groups == 0 && tid < kTcRows && tid < U.P_tile) {
       // no nodes in this split: its share of the tile is zero
       float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
@@ -775,7 +790,6 @@ struct TcPlan {
   TcItem *items;
   int *nf, *ng, *of, *og;
   int *error;
-  float *scratch;
   float2 *partials;
   int max_splits;
 };
@@ -801,7 +815,6 @@ static void carve_tc(Carve &c, const fm_signal_args *a, TcPlan &pl) {
   pl.of = c.take<int>(S + 2);
   pl.og = c.take<int>(S + 2);
   pl.error = c.take<int>(4);
-  pl.scratch = c.take<float>((size_t)kSmCount * kTcRows * 256);
   pl.max_splits = tc_max_splits(S, V);
   pl.partials = c.take<float2>((size_t)pl.max_splits * S * V);
 }
@@ -882,7 +895,6 @@ int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
     p.plan = pl.runs.counts;
     p.partials = pl.partials;
     p.out = out;
-    p.scratch = pl.scratch;
     p.error = pl.runs.error;
 
     ScopedTimer timer(ctx, "signal_tc");
