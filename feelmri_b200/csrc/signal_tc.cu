@@ -506,7 +506,78 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     }
     const uint32_t g0 = gst;
     int next_drain = 0;
-    if (a_role) {
+    if (!fac) {
+      // ------------------------------------------- generic unit, all warps --
+      // B is only the weights of the unit's VG columns (NT = 16), so every
+      // warp writes A: rows 32 (w % 4) + lane, nodes 4 (w / 4) .. + 3 of a
+      // stage; threads 0-127 also write one B element (pair tid % 8, node
+      // tid / 8).  Pairs past VG hold values no output reads.
+      const int grow = (warp & 3) * 32 + lane, gc = warp >> 2;
+      double gx = 0, gy = 0, gz = 0;
+      if (grow < U.P_tile) {
+        const int s_p = U.run.start + U.it.p0 + grow;
+        gx = p.kx[s_p];
+        gy = p.ky[s_p];
+        gz = p.kz[s_p];
+      }
+      const bool g_active = (warp & 3) * 32 < U.P_tile;
+      const uint32_t ga0 = L.a_hi + kmajor_offset(grow, 8 * gc, kTcRows);
+      const uint32_t gl0 = L.a_lo + kmajor_offset(grow, 8 * gc, kTcRows);
+      const int gpair = tid & 7, gnode = tid >> 3;
+      const bool g_b = tid < kTcRows && gpair < NH;
+      const int gv = gpair < VG ? gpair : 0;
+      const uint32_t gbr = kmajor_offset(gpair, 2 * gnode, NT), gbi = kmajor_offset(NH + gpair, 2 * gnode, NT);
+      for (uint32_t st = 0; st < nst; ++st) {
+        const uint32_t g = g0 + st, s = g & (kTcStages - 1);
+        const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
+        if (loader && blk + 1 < n_blocks && (j == 4 || j == 6)) {
+          const int64_t n1 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes + tid;
+          if (j == 4) {
+            if (n1 < U.n_end) tc_load_raw(p, n1, raw);
+          } else {
+            tc_derive(p, U, n1, raw, wrun, tg, pos_all + (buf ^ 1) * 3 * kTcBlockNodes,
+                      w_all + (buf ^ 1) * VG * kWStride, tid);
+          }
+        }
+        tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
+        ptx::named_barrier(1, kTcProducers);
+        if (issuer && st > 0)
+          tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g - 1, st - 1, nst);
+        const uint32_t stg = sbase + s * L.stage_bytes;
+        if (g_active) {
+          const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 4 * gc;
+          uint32_t h[4], l[4];
+#pragma unroll
+          for (int u4 = 0; u4 < 4; u4 += 2) {
+            const double2 x = *reinterpret_cast<const double2 *>(px + u4);
+            const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
+            const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
+            float c0, s0, c1, s1;
+            cycles_cos_sin(fma(gz, z.x, fma(gy, y.x, gx * x.x)), c0, s0);
+            cycles_cos_sin(fma(gz, z.y, fma(gy, y.y, gx * x.y)), c1, s1);
+            split_pair(c0, s0, h[u4], l[u4]);
+            split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
+          }
+          st_shared_v4(stg + ga0, h[0], h[1], h[2], h[3]);
+          st_shared_v4(stg + gl0, l[0], l[1], l[2], l[3]);
+        }
+        if (g_b) {
+          const float2 wv = w_all[(buf * VG + gv) * kWStride + j * kTcNodes + gnode];
+          uint32_t hb, lb;
+          split_pair(wv.x, wv.y, hb, lb);
+          const uint32_t hm = __byte_perm(hb, 0u, 0x1032) ^ 0x80000000u, lm = __byte_perm(lb, 0u, 0x1032) ^ 0x80000000u;
+          asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_hi + gbr), "r"(hb));
+          asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_lo + gbr), "r"(lb));
+          asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_hi + gbi), "r"(hm));
+          asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_lo + gbi), "r"(lm));
+        }
+        ptx::fence_proxy_async_smem();
+        if ((st & (kTcDrain - 1)) == 0 && st > 0) {
+          tc_fold(p, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
+          ++next_drain;
+        }
+      }
+    } else if (a_role) {
       // ------------------------------------------------------- A rows --
       const bool active = (rw >> 1) * 32 < U.P_tile;
       for (uint32_t st = 0; st < nst; ++st) {
