@@ -138,6 +138,11 @@ class MassArgs(C.Structure):
 
 
 # name -> (restype, argtypes)
+class TcTuning(C.Structure):
+    """fm_tc_tuning: work-unit shape of the batched tensor-core Signal."""
+    _fields_ = [("split_nodes", C.c_int32), ("kz_cap", C.c_int32), ("reserved", C.c_int32 * 2)]
+
+
 SIGNATURES = {
     "fm_ctx_create": (C.c_int, [C.c_int, C.POINTER(_p)]),
     "fm_ctx_destroy": (C.c_int, [_p]),
@@ -162,6 +167,9 @@ SIGNATURES = {
     "fm_signal_status": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, _p, C.c_size_t]),
     "fm_signal_workspace_size": (C.c_int, [C.POINTER(SignalArgs), C.c_int, C.POINTER(C.c_size_t)]),
     "fm_signal_count_time_runs": (C.c_int64, [_p, _i64, C.c_int]),
+    "fm_signal_batch_workspace_size": (C.c_int, [C.POINTER(SignalArgs), C.c_int, C.POINTER(C.c_size_t)]),
+    "fm_signal_batch_enqueue": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, C.POINTER(TcTuning), _p, C.c_size_t]),
+    "fm_signal_batch_status": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, _p, C.c_size_t]),
     "fm_mass_assemble": (C.c_int, [_p, C.POINTER(MassArgs), C.c_int, C.POINTER(_i64), _p, _p, _p, _i64, _p,
                                    C.c_size_t]),
     "fm_mass_lumped": (C.c_int, [_p, C.POINTER(MassArgs), C.c_int, _p, _p, C.c_size_t]),

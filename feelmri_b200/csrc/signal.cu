@@ -12,6 +12,10 @@ size_t tc_workspace(const fm_signal_args *a);
 template <typename T>
 int signal_plain_errors(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes);
 int signal_tc_errors(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes);
+int signal_tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc_tuning *tune, void *ws,
+                    size_t ws_bytes);
+int signal_tc_batch_errors(fm_ctx *ctx, const fm_signal_args *probs, int n, void *ws, size_t ws_bytes);
+size_t tc_batch_workspace_size(const fm_signal_args *probs, int n);
 
 int validate_signal(const fm_signal_args *a, const char *who) {
   FM_REQUIRE(a != nullptr, FM_ERR_ARG, "%s: null args", who);
@@ -95,6 +99,40 @@ int fm_signal_status(fm_ctx *ctx, const fm_signal_args *a, int precision, void *
 int fm_signal(fm_ctx *ctx, const fm_signal_args *a, int precision, void *ws, size_t ws_bytes) {
   FM_TRY(fm_signal_enqueue(ctx, a, precision, ws, ws_bytes));
   return fm_signal_status(ctx, a, precision, ws, ws_bytes);
+}
+
+static int validate_batch(const fm_signal_args *probs, int n, const char *who) {
+  FM_REQUIRE(n >= 0, FM_ERR_SHAPE, "%s: negative problem count", who);
+  FM_REQUIRE(n == 0 || probs != nullptr, FM_ERR_ARG, "%s: null problem array", who);
+  for (int i = 0; i < n; ++i) FM_TRY(validate_signal(&probs[i], who));
+  return FM_OK;
+}
+
+int fm_signal_batch_workspace_size(const fm_signal_args *probs, int n, size_t *bytes) {
+  FM_REQUIRE(bytes != nullptr, FM_ERR_ARG, "fm_signal_batch_workspace_size: null output");
+  FM_TRY(validate_batch(probs, n, "fm_signal_batch_workspace_size"));
+  *bytes = tc_batch_workspace_size(probs, n);
+  return FM_OK;
+}
+
+int fm_signal_batch_enqueue(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc_tuning *tune, void *ws,
+                            size_t ws_bytes) {
+  FM_TRY(ctx_ok(ctx));
+  FM_TRY(validate_batch(probs, n, "fm_signal_batch_enqueue"));
+  if (tune) {
+    FM_REQUIRE(tune->split_nodes >= 0 && tune->kz_cap >= 0, FM_ERR_ARG,
+               "fm_signal_batch_enqueue: negative tuning value");
+  }
+  DeviceGuard g(ctx->device);
+  FM_REQUIRE(g.ok, FM_ERR_CUDA, "fm_signal_batch_enqueue: cannot select device %d", ctx->device);
+  return signal_tc_batch(ctx, probs, n, tune, ws, ws_bytes);
+}
+
+int fm_signal_batch_status(fm_ctx *ctx, const fm_signal_args *probs, int n, void *ws, size_t ws_bytes) {
+  FM_TRY(ctx_ok(ctx));
+  FM_TRY(validate_batch(probs, n, "fm_signal_batch_status"));
+  DeviceGuard g(ctx->device);
+  return signal_tc_batch_errors(ctx, probs, n, ws, ws_bytes);
 }
 
 int64_t fm_signal_count_time_runs(const void *t_host, int64_t n_samples, int is_double) {

@@ -31,6 +31,7 @@
 // range).  All waits are bounded: on timeout the block records an error,
 // lets its MMAs finish and frees its tensor memory.
 #include <cmath>
+#include <vector>
 #include <cub/cub.cuh>
 
 #include "signal_common.cuh"
@@ -46,7 +47,6 @@ constexpr int kTcStagesPerBlock = kTcBlockNodes / kTcNodes;
 constexpr int kTcProducerWarps = 16;
 constexpr int kTcProducers = 32 * kTcProducerWarps;  // every thread of the block
 constexpr int kTcThreads = kTcProducers;
-constexpr int kTcIssuer = 96;       // thread that issues the MMAs (warp 3: A rows 96-127)
 constexpr int kTcVGroup = 8;        // Mxy columns per launch
 // Stages accumulated in the tensor-memory accumulator before it is folded
 // into an FP32 round-to-nearest running sum (also in tensor memory).  The
@@ -77,21 +77,31 @@ struct TcDev {
   const double *run_t;
   const TcRun *runs;
   const TcItem *items;
-  int Qt, NT, acc_cols;
+  int Qt, NT, kind;  // kind 0: factored runs, 1: generic runs
   const int *plan;  // device: [2] factored items, [3] generic items, [4] splits, [5] nodes per split
   float2 *partials; // (splits, S, V) when splits > 1
   float2 *out;
   int *error;
 };
 
-// Work list of one launch, read from the device-side plan.
+// One launch works through a table of entries (one per problem, Mxy column
+// group and run kind); the device-side plan gives each entry's units.
+struct TcBatchDev {
+  const TcDev *entries;
+  const int *offsets;  // device: n_entries + 1 running unit counts
+  int n_entries;
+  int acc_cols;  // tensor-memory columns of the widest entry (accumulator; the running sum follows)
+};
+
+// Work list of one entry, read from the device-side plan.
 struct TcWork {
   int splits, item0, n_items;
   int64_t chunk;
   float2 *out;
 };
 
-__device__ inline TcWork tc_work(const TcDev &p, int kind) {
+__device__ inline TcWork tc_work(const TcDev &p) {
+  const int kind = p.kind;
   TcWork W;
   W.splits = p.plan[4];
   W.chunk = p.plan[5];
@@ -107,9 +117,14 @@ __device__ inline TcWork tc_work(const TcDev &p, int kind) {
 constexpr int kWStride = kTcBlockNodes + 2;
 constexpr int kEStride = kTcNodes + 2;
 
+// Barriers and the tensor-memory address live in the first kTcFront bytes
+// (fixed, since the tile layout after them changes from unit to unit).
+constexpr uint32_t kTcFront = 1024;
+constexpr uint32_t kTcBars = 0, kTcMisc = 128;
+
 struct TcSmem {
   uint32_t stage_bytes, a_hi, a_lo, b_hi, b_lo;  // offsets inside a stage
-  uint32_t pos, w, etab, bars, misc, total;
+  uint32_t stages, pos, w, etab, total;
 };
 
 // Node data is double-buffered: block b is read while block b + 1 is written.
@@ -120,17 +135,14 @@ __host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
   L.b_hi = 2 * kAStageBytes;
   L.b_lo = 2 * kAStageBytes + NT * 2 * kTcNodes * 2;
   L.stage_bytes = 2 * kAStageBytes + 2 * NT * 2 * kTcNodes * 2;
-  uint32_t off = kTcStages * L.stage_bytes;
+  L.stages = kTcFront;
+  uint32_t off = kTcFront + kTcStages * L.stage_bytes;
   L.pos = off;  // [2][3][128] double: x, y, z of the moved nodes
   off += 2 * 3 * kTcBlockNodes * 8;
   L.w = off;  // [2][VG][kWStride] float2
   off += 2 * VG * kWStride * 8;
   L.etab = off;  // [2][Qt][kEStride] float2, by stage parity
   off += 2 * Qt * kEStride * 8;
-  L.bars = off;
-  off += 8 * 8;
-  L.misc = off;  // tmem address, abort flag
-  off += 16;
   L.total = off;
   return L;
 }
@@ -285,7 +297,7 @@ __device__ inline void tc_phase_pair(const double *pb, float2 *et, int q, int n0
 // in FP32 round-to-nearest.  Warp w handles TMEM lanes of quarter w % 4 and
 // column quarter w / 4.  The next MMA into the accumulator is issued after a
 // block barrier.
-__device__ inline void tc_fold(const TcDev &p, uint64_t *accfull, uint32_t tmem, int gg, bool first,
+__device__ inline void tc_fold(const TcDev &p, int acc_cols, uint64_t *accfull, uint32_t tmem, int gg, bool first,
                                volatile int *abort_flag) {
   const int warp = threadIdx.x >> 5;
   tc_wait(accfull, gg & 1, abort_flag);
@@ -302,7 +314,7 @@ __device__ inline void tc_fold(const TcDev &p, uint64_t *accfull, uint32_t tmem,
       uint32_t r[8];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        ptx::tmem_ld8(tmem + lanes + (uint32_t)(p.acc_cols + c0 + 8 * h), r);
+        ptx::tmem_ld8(tmem + lanes + (uint32_t)(acc_cols + c0 + 8 * h), r);
         ptx::tmem_wait_ld();
 #pragma unroll
         for (int i = 0; i < 8; ++i)
@@ -311,7 +323,7 @@ __device__ inline void tc_fold(const TcDev &p, uint64_t *accfull, uint32_t tmem,
     } else {
       ptx::tmem_wait_ld();
     }
-    ptx::tmem_st16(tmem + lanes + (uint32_t)(p.acc_cols + c0), a);
+    ptx::tmem_st16(tmem + lanes + (uint32_t)(acc_cols + c0), a);
   }
   ptx::tmem_wait_st();
   ptx::tc_fence_before();
@@ -320,8 +332,8 @@ __device__ inline void tc_fold(const TcDev &p, uint64_t *accfull, uint32_t tmem,
 // Writes the unit's result: running sum (when earlier groups were folded) +
 // accumulator of the last group gg, to the output samples.  Warp w reads TMEM
 // lanes of quarter w % 4 and every fourth chunk of 8 pairs starting at w / 4.
-__device__ inline void tc_final(const TcDev &p, const TcWork &W, const TcUnit &U, uint64_t *accfull, uint32_t tmem,
-                                int gg, bool has_sum, volatile int *abort_flag) {
+__device__ inline void tc_final(const TcDev &p, int acc_cols, const TcWork &W, const TcUnit &U, uint64_t *accfull,
+                                uint32_t tmem, int gg, bool has_sum, volatile int *abort_flag) {
   const int tid = threadIdx.x, warp = tid >> 5;
   tc_wait(accfull, gg & 1, abort_flag);
   ptx::tc_fence_after();
@@ -337,8 +349,8 @@ __device__ inline void tc_final(const TcDev &p, const TcWork &W, const TcUnit &U
     ptx::tmem_ld8(taddr + (uint32_t)c0, r);
     ptx::tmem_ld8(taddr + (uint32_t)(NH + c0), m);
     if (has_sum) {
-      ptx::tmem_ld8(taddr + (uint32_t)(p.acc_cols + c0), sr);
-      ptx::tmem_ld8(taddr + (uint32_t)(p.acc_cols + NH + c0), sm);
+      ptx::tmem_ld8(taddr + (uint32_t)(acc_cols + c0), sr);
+      ptx::tmem_ld8(taddr + (uint32_t)(acc_cols + NH + c0), sm);
     }
     ptx::tmem_wait_ld();
     if (!row_ok) continue;
@@ -367,7 +379,7 @@ __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, 
   const uint32_t s = g % kTcStages;
   const bool group_start = (st % kTcDrain) == 0;
   ptx::tc_fence_after();
-  const uint32_t stage = sbase + s * L.stage_bytes;
+  const uint32_t stage = sbase + L.stages + s * L.stage_bytes;
   const uint32_t acc = tmem;
 #pragma unroll
   for (int ks = 0; ks < 2; ++ks) {
@@ -383,24 +395,18 @@ __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, 
   if ((st % kTcDrain) == kTcDrain - 1 || st == n_stages - 1) ptx::mma_commit(accfull);
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_constant__ TcDev p, int kind) {
+__global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_constant__ TcBatchDev B) {
   extern __shared__ __align__(1024) unsigned char smem[];
   // work sizes come from the device-side plan, so the launch needs no host
   // synchronisation (and can be captured in a CUDA graph)
-  const TcWork W = tc_work(p, kind);
-  const int n_units = W.n_items * W.splits;
+  const int n_units = B.offsets[B.n_entries];
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  const int NT = p.NT, NH = NT >> 1, VG = p.VG, Qt = p.Qt;
-  const TcSmem L = tc_smem_layout(NT, VG, Qt);
-  uint64_t *empty = reinterpret_cast<uint64_t *>(smem + L.bars);
+  uint64_t *empty = reinterpret_cast<uint64_t *>(smem + kTcBars);
   uint64_t *accfull = empty + kTcStages;
   uint64_t *done = accfull + 1;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L.misc);
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + L.misc + 4);
-  double *pos_all = reinterpret_cast<double *>(smem + L.pos);
-  float2 *w_all = reinterpret_cast<float2 *>(smem + L.w);
-  float2 *etab = reinterpret_cast<float2 *>(smem + L.etab);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kTcMisc);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + kTcMisc + 4);
   const uint32_t sbase = ptx::smem_addr(smem);
 
   if (tid == 0) {
@@ -410,12 +416,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     *abort_flag = 0;
     ptx::fence_mbar_init();
   }
-  if (warp == 0) ptx::tmem_alloc(tmem_slot, 2 * p.acc_cols);
+  if (warp == 0) ptx::tmem_alloc(tmem_slot, 2 * B.acc_cols);
   ptx::tc_fence_before();
   __syncthreads();
   ptx::tc_fence_after();
   const uint32_t tmem = tmem_slot[0];
-  const uint32_t idesc = ptx::idesc_bf16_f32(kTcRows, NT);
 
   // Roles (warp-uniform).  Warps 0-7 write A: rows 32 (w >> 1) + lane, nodes
   // 8 (w & 1) .. + 7 of every stage.  Warps 8-15 write B: pairs
@@ -430,31 +435,36 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   const int half = rw & 1;                // nodes 8 half .. 8 half + 7 of a stage
   const bool loader = tid < kTcBlockNodes;
   const bool issuer = tid == 7 * 32;
-  // operand addresses inside a stage (K chunks 2 half and 2 half + 1 of 8)
-  uint32_t o_hi0, o_hi1, o_lo0, o_lo1, o_ih0 = 0, o_ih1 = 0, o_il0 = 0, o_il1 = 0;
-  if (a_role) {
-    o_hi0 = L.a_hi + kmajor_offset(row, 16 * half, kTcRows);
-    o_hi1 = L.a_hi + kmajor_offset(row, 16 * half + 8, kTcRows);
-    o_lo0 = L.a_lo + kmajor_offset(row, 16 * half, kTcRows);
-    o_lo1 = L.a_lo + kmajor_offset(row, 16 * half + 8, kTcRows);
-  } else {
-    o_hi0 = L.b_hi + kmajor_offset(row, 16 * half, NT);
-    o_hi1 = L.b_hi + kmajor_offset(row, 16 * half + 8, NT);
-    o_lo0 = L.b_lo + kmajor_offset(row, 16 * half, NT);
-    o_lo1 = L.b_lo + kmajor_offset(row, 16 * half + 8, NT);
-    o_ih0 = L.b_hi + kmajor_offset(NH + row, 16 * half, NT);
-    o_ih1 = L.b_hi + kmajor_offset(NH + row, 16 * half + 8, NT);
-    o_il0 = L.b_lo + kmajor_offset(NH + row, 16 * half, NT);
-    o_il1 = L.b_lo + kmajor_offset(NH + row, 16 * half + 8, NT);
-  }
-  const bool b_rows = row < NH;
   // phase-table thread: q = (tid - 256) / 8 (+ 32), nodes 2 ((tid - 256) % 8) + {0, 1}
   const int tq = (tid - 256) >> 3, tn = ((tid - 256) & 7) * 2;
   uint32_t gst = 0;
   int gbase = 0;
   TcRaw raw;
   for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
-    const TcUnit U = tc_unit(p, W, u);
+    // the unit's entry: offsets[e] <= u < offsets[e + 1]
+    int e_lo = 0, e_hi = B.n_entries;
+    while (e_hi - e_lo > 1) {
+      const int mid = (e_lo + e_hi) >> 1;
+      if (B.offsets[mid] <= u) e_lo = mid; else e_hi = mid;
+    }
+    const TcDev &p = B.entries[e_lo];
+    const TcWork W = tc_work(p);
+    const int NT = p.NT, NH = NT >> 1, VG = p.VG, Qt = p.Qt;
+    const TcSmem L = tc_smem_layout(NT, VG, Qt);
+    double *pos_all = reinterpret_cast<double *>(smem + L.pos);
+    float2 *w_all = reinterpret_cast<float2 *>(smem + L.w);
+    float2 *etab = reinterpret_cast<float2 *>(smem + L.etab);
+    const uint32_t sstages = sbase + L.stages;
+    const uint32_t idesc = ptx::idesc_bf16_f32(kTcRows, NT);
+    // operand addresses inside a stage: the thread's first 8-K chunk; the
+    // second chunk is 128 bytes on, the lo tile d_lo bytes on and (B) the
+    // imaginary row block d_im bytes on
+    const uint32_t o_hi = a_role ? L.a_hi + kmajor_offset(row, 16 * half, kTcRows)
+                                 : L.b_hi + kmajor_offset(row, 16 * half, NT);
+    const uint32_t d_lo = a_role ? L.a_lo - L.a_hi : L.b_lo - L.b_hi;
+    const uint32_t d_im = (uint32_t)(NH >> 3) * 256;
+    const bool b_rows = row < NH;
+    const TcUnit U = tc_unit(p, W, u - B.offsets[e_lo]);
     const bool fac = U.run.factored != 0;
     const uint32_t nst = (uint32_t)U.n_stages;
     ptx::named_barrier(1, kTcProducers);  // the previous unit's readers are done
@@ -543,7 +553,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         ptx::named_barrier(1, kTcProducers);
         if (issuer && st > 0)
           tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g - 1, st - 1, nst);
-        const uint32_t stg = sbase + s * L.stage_bytes;
+        const uint32_t stg = sstages + s * L.stage_bytes;
         if (g_active) {
           const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 4 * gc;
           uint32_t h[4], l[4];
@@ -573,7 +583,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         }
         ptx::fence_proxy_async_smem();
         if ((st & (kTcDrain - 1)) == 0 && st > 0) {
-          tc_fold(p, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
+          tc_fold(p, B.acc_cols, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
       }
@@ -605,7 +615,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g - 1, st - 1, nst);
         if (active) {
           // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n
-          const uint32_t stg = sbase + s * L.stage_bytes;
+          const uint32_t stg = sstages + s * L.stage_bytes;
           const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 8 * half;
           uint32_t h[8], l[8];
 #pragma unroll
@@ -619,17 +629,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
             split_pair(c0, s0, h[u4], l[u4]);
             split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
           }
-          st_shared_v4(stg + o_hi0, h[0], h[1], h[2], h[3]);
-          st_shared_v4(stg + o_hi1, h[4], h[5], h[6], h[7]);
-          st_shared_v4(stg + o_lo0, l[0], l[1], l[2], l[3]);
-          st_shared_v4(stg + o_lo1, l[4], l[5], l[6], l[7]);
+          const uint32_t a_st = stg + o_hi;
+          st_shared_v4(a_st, h[0], h[1], h[2], h[3]);
+          st_shared_v4(a_st + 128, h[4], h[5], h[6], h[7]);
+          st_shared_v4(a_st + d_lo, l[0], l[1], l[2], l[3]);
+          st_shared_v4(a_st + d_lo + 128, l[4], l[5], l[6], l[7]);
         }
         ptx::fence_proxy_async_smem();
         // the previous group's last MMAs went out at this stage's barrier:
         // fold the accumulator into the running sum before the next group
         // starts (its first MMAs go out at the next stage's barrier)
         if ((st & (kTcDrain - 1)) == 0 && st > 0) {
-          tc_fold(p, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
+          tc_fold(p, B.acc_cols, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
       }
@@ -670,15 +681,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           lm[i] = __byte_perm(lr[i], 0u, 0x1032) ^ 0x80000000u;
         }
         if (b_rows) {
-          const uint32_t stg = sbase + s * L.stage_bytes;
-          st_shared_v4(stg + o_hi0, hr[0], hr[1], hr[2], hr[3]);
-          st_shared_v4(stg + o_hi1, hr[4], hr[5], hr[6], hr[7]);
-          st_shared_v4(stg + o_lo0, lr[0], lr[1], lr[2], lr[3]);
-          st_shared_v4(stg + o_lo1, lr[4], lr[5], lr[6], lr[7]);
-          st_shared_v4(stg + o_ih0, hm[0], hm[1], hm[2], hm[3]);
-          st_shared_v4(stg + o_ih1, hm[4], hm[5], hm[6], hm[7]);
-          st_shared_v4(stg + o_il0, lm[0], lm[1], lm[2], lm[3]);
-          st_shared_v4(stg + o_il1, lm[4], lm[5], lm[6], lm[7]);
+          const uint32_t stg = sstages + s * L.stage_bytes;
+          const uint32_t b_st = stg + o_hi;
+          st_shared_v4(b_st, hr[0], hr[1], hr[2], hr[3]);
+          st_shared_v4(b_st + 128, hr[4], hr[5], hr[6], hr[7]);
+          st_shared_v4(b_st + d_lo, lr[0], lr[1], lr[2], lr[3]);
+          st_shared_v4(b_st + d_lo + 128, lr[4], lr[5], lr[6], lr[7]);
+          st_shared_v4(b_st + d_im, hm[0], hm[1], hm[2], hm[3]);
+          st_shared_v4(b_st + d_im + 128, hm[4], hm[5], hm[6], hm[7]);
+          st_shared_v4(b_st + d_im + d_lo, lm[0], lm[1], lm[2], lm[3]);
+          st_shared_v4(b_st + d_im + d_lo + 128, lm[4], lm[5], lm[6], lm[7]);
         }
         // next stage's phase table into the other parity buffer: its last
         // readers (stage st - 1) are past this stage's barrier
@@ -692,7 +704,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         }
         ptx::fence_proxy_async_smem();
         if ((st & (kTcDrain - 1)) == 0 && st > 0) {
-          tc_fold(p, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
+          tc_fold(p, B.acc_cols, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
       }
@@ -703,7 +715,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       if (issuer)
         tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, gst - 1, nst - 1, nst);
     }
-    if (U.n_groups > 0) tc_final(p, W, U, accfull, tmem, gbase + U.n_groups - 1, U.n_groups > 1, abort_flag);
+    if (U.n_groups > 0) tc_final(p, B.acc_cols, W, U, accfull, tmem, gbase + U.n_groups - 1, U.n_groups > 1, abort_flag);
     if (U.n_groups == 0 && tid < kTcRows && tid < U.P_tile) {
       // no nodes in this split: its share of the tile is zero
       float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
@@ -720,10 +732,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   }
   ptx::tc_fence_before();
   __syncthreads();
-  if (tid == 0 && *abort_flag) atomicOr(p.error, kErrTimeout);
+  // a wait that ran out is reported for every problem of the launch
+  if (*abort_flag)
+    for (int e = tid; e < B.n_entries; e += kTcThreads) atomicOr(B.entries[e].error, kErrTimeout);
   if (warp == 0) {
     ptx::tc_fence_after();
-    ptx::tmem_dealloc(tmem, 2 * p.acc_cols);
+    ptx::tmem_dealloc(tmem, 2 * B.acc_cols);
   }
 }
 
@@ -784,14 +798,17 @@ __global__ void tc_count_kernel(const TcRun *__restrict__ runs, const int *__res
   ng[g] = r.factored ? 0 : items;
 }
 
-__global__ void tc_fill_kernel(const TcRun *__restrict__ runs, int *__restrict__ counts, int Qt,
-                               const int *__restrict__ of, const int *__restrict__ og, TcItem *__restrict__ items) {
+// Items of one Mxy column group: factored first, then generic; their counts
+// go to plan[2] and plan[3].
+__global__ void tc_fill_kernel(const TcRun *__restrict__ runs, const int *__restrict__ counts, int Qt,
+                               const int *__restrict__ of, const int *__restrict__ og, TcItem *__restrict__ items,
+                               int *__restrict__ plan) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = counts[0];
   if (g > n) return;
   if (g == n) {
-    counts[2] = of[n];
-    counts[3] = og[n];
+    plan[2] = of[n];
+    plan[3] = og[n];
     return;
   }
   const TcRun r = runs[g];
@@ -830,11 +847,51 @@ __host__ __device__ inline int tc_choose_splits(int64_t items, int64_t N, int ma
   return best;
 }
 
-__global__ void tc_plan_kernel(int *__restrict__ counts, int64_t N, int max_splits) {
+// Splits of one problem, shared by all its column groups (plan rows of 8
+// ints): from the node count per split when tuned, else balanced over the SMs.
+__global__ void tc_plan_kernel(int *__restrict__ plan, int n_groups, int64_t N, int max_splits, int split_nodes) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const int splits = tc_choose_splits((int64_t)counts[2] + counts[3], N, max_splits);
-  counts[4] = splits;
-  counts[5] = (int)(ceil_div(ceil_div(N, splits), kTcNodes) * kTcNodes);
+  int64_t items = 0;
+  for (int g = 0; g < n_groups; ++g) items += plan[8 * g + 2] + plan[8 * g + 3];
+  int splits;
+  if (split_nodes > 0) {
+    const int64_t s = ceil_div(N, (int64_t)split_nodes);
+    splits = (int)(s < 1 ? 1 : (s > max_splits ? max_splits : s));
+  } else {
+    splits = tc_choose_splits(items, N, max_splits);
+  }
+  const int chunk = (int)(ceil_div(ceil_div(N, splits), kTcNodes) * kTcNodes);
+  for (int g = 0; g < n_groups; ++g) {
+    plan[8 * g + 4] = splits;
+    plan[8 * g + 5] = chunk;
+  }
+}
+
+// Running unit counts of the launch's entries.
+__global__ void tc_batch_plan_kernel(const TcDev *__restrict__ entries, int n, int *__restrict__ offsets) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int acc = 0;
+  offsets[0] = 0;
+  for (int e = 0; e < n; ++e) {
+    const int *pl = entries[e].plan;
+    acc += (entries[e].kind == 0 ? pl[2] : pl[3]) * pl[4];
+    offsets[e + 1] = acc;
+  }
+}
+
+constexpr int kTcEntriesPerWrite = 16;
+struct TcEntryChunk {
+  TcDev e[kTcEntriesPerWrite];
+  int n;
+};
+
+// Copies entry descriptors (passed by value) to device memory, so that the
+// launch sequence holds no pointer to host memory and can be captured.
+__global__ void tc_write_entries_kernel(const __grid_constant__ TcEntryChunk c, TcDev *__restrict__ dst) {
+  const int words = c.n * (int)(sizeof(TcDev) / 4);
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(c.e);
+  uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+  for (int i = threadIdx.x; i < words; i += blockDim.x) d[i] = src[i];
 }
 
 __global__ void tc_reduce_kernel(const float2 *__restrict__ part, const int *__restrict__ plan, int64_t count,
@@ -852,17 +909,18 @@ __global__ void tc_reduce_kernel(const float2 *__restrict__ part, const int *__r
   out[e] = acc;
 }
 
+// Workspace of one problem.
 struct TcPlan {
   float *MM;
   Csr csr;
   Runs runs;
   float *weights;
   TcRun *tcruns;
-  TcItem *items;
+  TcItem *items;  // n_groups lists of 2 S + 2
   int *nf, *ng, *of, *og;
-  int *error;
+  int *plan;      // n_groups rows of 8 ints
   float2 *partials;
-  int max_splits;
+  int n_groups, max_splits;
 };
 
 static int tc_max_splits(int64_t S, int64_t V) {
@@ -872,45 +930,78 @@ static int tc_max_splits(int64_t S, int64_t V) {
   return (int)(s < 1 ? 1 : s);
 }
 
+static int tc_groups(int64_t V) { return (int)ceil_div(V, (int64_t)kTcVGroup); }
+
 static void carve_tc(Carve &c, const fm_signal_args *a, TcPlan &pl) {
   const int64_t S = a->n_ro * a->n_lines * a->n_kz;
   const int64_t N = a->n_nodes, V = a->n_vencs;
+  pl.n_groups = tc_groups(V);
   pl.MM = c.take<float>((size_t)N * V * 2);
   carve_csr(c, a->m_rows, a->m_nnz, pl.csr);
   carve_runs(c, S, kTcRows, pl.runs);
   pl.weights = c.take<float>((size_t)(S + 1) * motion_slots(a->motion));
   pl.tcruns = c.take<TcRun>(S + 1);
-  pl.items = c.take<TcItem>(2 * S + 2);
+  pl.items = c.take<TcItem>((size_t)pl.n_groups * (2 * S + 2));
   pl.nf = c.take<int>(S + 2);
   pl.ng = c.take<int>(S + 2);
   pl.of = c.take<int>(S + 2);
   pl.og = c.take<int>(S + 2);
-  pl.error = c.take<int>(4);
+  pl.plan = c.take<int>((size_t)8 * (pl.n_groups > 0 ? pl.n_groups : 1));
   pl.max_splits = tc_max_splits(S, V);
   pl.partials = c.take<float2>((size_t)pl.max_splits * S * V);
 }
 
-size_t tc_workspace(const fm_signal_args *a) {
+// Entries of a launch: per problem, per column group, both run kinds.
+static int tc_n_entries(const fm_signal_args *probs, int n) {
+  int e = 0;
+  for (int i = 0; i < n; ++i) e += 2 * tc_groups(probs[i].n_vencs);
+  return e;
+}
+
+static void carve_batch(Carve &c, const fm_signal_args *probs, int n, TcPlan *plans, TcDev **entries,
+                        int **offsets) {
+  for (int i = 0; i < n; ++i) carve_tc(c, &probs[i], plans[i]);
+  const int ne = tc_n_entries(probs, n);
+  *entries = c.take<TcDev>(ne > 0 ? ne : 1);
+  *offsets = c.take<int>(ne + 1);
+}
+
+// Tile shape of a column group: up to 128 (q, v) pairs per tile and at most
+// 64 kz values (fewer when tuned).
+static int tc_qt(const fm_signal_args *a, int VG, const fm_tc_tuning *tune) {
+  int cap = (128 / VG < 64) ? 128 / VG : 64;
+  if (tune && tune->kz_cap > 0 && tune->kz_cap < cap) cap = tune->kz_cap;
+  return (int)((a->n_kz < cap) ? a->n_kz : cap);
+}
+
+static void tc_shape(int Qt, int VG, int &NT, int &acc_cols) {
+  NT = (int)ceil_div(2 * Qt * VG, 16) * 16;
+  acc_cols = 32;
+  while (acc_cols < NT) acc_cols <<= 1;
+}
+
+static size_t tc_batch_workspace(const fm_signal_args *probs, int n) {
   Carve c(nullptr, 0);
-  TcPlan pl;
-  carve_tc(c, a, pl);
+  std::vector<TcPlan> plans(n > 0 ? n : 1);
+  TcDev *entries;
+  int *offsets;
+  carve_batch(c, probs, n, plans.data(), &entries, &offsets);
   return c.used;
 }
 
-int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
-  const char *who = "fm_signal(BF16X3)";
-  cudaStream_t st = ctx->stream;
+size_t tc_workspace(const fm_signal_args *a) { return tc_batch_workspace(a, 1); }
+
+// Preparation of one problem (runs, M Mxy, motion weights, run kinds, items
+// and splits); fills its launch entries.  Returns the number of entries.
+static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *tune, TcDev *host_entries,
+                      cudaStream_t st, const char *who) {
   const int64_t S = a->n_ro * a->n_lines * a->n_kz;
   const int64_t N = a->n_nodes, V = a->n_vencs;
-  Carve cv(ws, ws_bytes);
-  TcPlan pl;
-  carve_tc(cv, a, pl);
-  FM_TRY(carve_ok(cv, who));
-  if (S == 0 || V == 0) return FM_OK;
+  if (S == 0 || V == 0) return 0;
   float2 *out = static_cast<float2 *>(a->out);
   if (N == 0) {
     FM_CUDA(cudaMemsetAsync(out, 0, (size_t)S * V * sizeof(float2), st));
-    return FM_OK;
+    return 0;
   }
   FM_REQUIRE(a->n_lines * a->n_kz < (1LL << 30), FM_ERR_SHAPE, "%s: slab too large", who);
   const float *kx = static_cast<const float *>(a->kx), *ky = static_cast<const float *>(a->ky),
@@ -925,12 +1016,13 @@ int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
                                                            (int)a->n_lines, (int)a->n_kz, pl.tcruns);
   count_launch();
   FM_TRY(check_launch("tc_classify_kernel"));
-
-  for (int64_t v0 = 0; v0 < V; v0 += kTcVGroup) {
+  int ne = 0;
+  for (int g = 0; g < pl.n_groups; ++g) {
+    const int64_t v0 = (int64_t)g * kTcVGroup;
     const int VG = (int)((V - v0) < kTcVGroup ? (V - v0) : kTcVGroup);
-    // columns per tile: up to 128 (q, v) pairs and at most 64 kz values
-    const int q_cap = (128 / VG < 64) ? 128 / VG : 64;
-    const int Qt_f = (int)((a->n_kz < q_cap) ? a->n_kz : q_cap);
+    const int Qt_f = tc_qt(a, VG, tune);
+    TcItem *items = pl.items + (size_t)g * (2 * S + 2);
+    int *plan = pl.plan + 8 * g;
     const unsigned gb = (unsigned)ceil_div(S + 1, 256);
     tc_count_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.nf, pl.ng, S);
     count_launch();
@@ -940,63 +1032,143 @@ int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
     cb = pl.runs.cub_bytes;
     FM_CUDA(cub::DeviceScan::ExclusiveSum(pl.runs.cub_tmp, cb, pl.ng, pl.og, (int)(S + 1), st));
     count_launch(2);
-    tc_fill_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.of, pl.og, pl.items);
+    tc_fill_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.of, pl.og, items, plan);
     count_launch();
     FM_TRY(check_launch("tc_fill_kernel"));
-    tc_plan_kernel<<<1, 32, 0, st>>>(pl.runs.counts, N, pl.max_splits);
-    count_launch();
-    FM_TRY(check_launch("tc_plan_kernel"));
-
-    TcDev p{};
-    p.N = N; p.S = S; p.V = V;
-    p.v0 = (int)v0; p.VG = VG;
-    p.n_lines = (int)a->n_lines; p.n_kz = (int)a->n_kz;
-    p.kx = kx; p.ky = ky; p.kz = kz;
-    p.r0 = static_cast<const float *>(a->r0);
-    p.phi = static_cast<const float *>(a->phi);
-    p.T2 = static_cast<const float *>(a->T2);
-    p.MM = reinterpret_cast<const float2 *>(pl.MM);
-    p.md = md;
-    p.weights = (md.kind == FM_MOTION_TERMS) ? pl.weights : nullptr;
-    p.table = (a->motion && a->motion->kind == FM_MOTION_TABLE) ? static_cast<const float *>(a->motion->table)
-                                                                 : nullptr;
-    p.run_t = pl.runs.run_t;
-    p.runs = pl.tcruns;
-    p.items = pl.items;
-    p.plan = pl.runs.counts;
-    p.partials = pl.partials;
-    p.out = out;
-    p.error = pl.runs.error;
-
-    ScopedTimer timer(ctx, "signal_tc");
     for (int kind = 0; kind < 2; ++kind) {
+      TcDev &p = host_entries[ne++];
+      p = TcDev{};
+      p.N = N; p.S = S; p.V = V;
+      p.v0 = (int)v0; p.VG = VG;
+      p.n_lines = (int)a->n_lines; p.n_kz = (int)a->n_kz;
+      p.kx = kx; p.ky = ky; p.kz = kz;
+      p.r0 = static_cast<const float *>(a->r0);
+      p.phi = static_cast<const float *>(a->phi);
+      p.T2 = static_cast<const float *>(a->T2);
+      p.MM = reinterpret_cast<const float2 *>(pl.MM);
+      p.md = md;
+      p.weights = (md.kind == FM_MOTION_TERMS) ? pl.weights : nullptr;
+      p.table = (a->motion && a->motion->kind == FM_MOTION_TABLE) ? static_cast<const float *>(a->motion->table)
+                                                                   : nullptr;
+      p.run_t = pl.runs.run_t;
+      p.runs = pl.tcruns;
+      p.items = items;
+      p.plan = plan;
+      p.partials = pl.partials;
+      p.out = out;
+      p.error = pl.runs.error;
+      p.kind = kind;
       p.Qt = kind == 0 ? Qt_f : 1;
-      const int cols = 2 * p.Qt * VG;
-      p.NT = (int)ceil_div(cols, 16) * 16;
-      p.acc_cols = 32;
-      while (p.acc_cols < p.NT) p.acc_cols <<= 1;
-      const TcSmem Ls = tc_smem_layout(p.NT, VG, p.Qt);
-      const size_t smem = Ls.total + 1024;
-      FM_REQUIRE(smem <= 232448, FM_ERR_UNSUPPORTED, "%s: tile needs %zu bytes of shared memory", who, smem);
-      FM_CUDA(cudaFuncSetAttribute(signal_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      signal_tc_kernel<<<kSmCount, kTcThreads, smem, st>>>(p, kind);
-      count_launch();
-      FM_TRY(check_launch("signal_tc_kernel"));
+      int acc_cols;
+      tc_shape(p.Qt, VG, p.NT, acc_cols);
     }
-    const int64_t count = S * V;
-    tc_reduce_kernel<<<(unsigned)ceil_div(count, 256), 256, 0, st>>>(pl.partials, pl.runs.counts, count, out);
+  }
+  tc_plan_kernel<<<1, 32, 0, st>>>(pl.plan, pl.n_groups, N, pl.max_splits, tune ? tune->split_nodes : 0);
+  count_launch();
+  FM_TRY(check_launch("tc_plan_kernel"));
+  return ne;
+}
+
+// Signal for n problems: per-problem preparation, then one persistent
+// tensor-core launch over all of their work units, then the split sums.
+static int tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc_tuning *tune, void *ws,
+                    size_t ws_bytes, const char *who) {
+  cudaStream_t st = ctx->stream;
+  Carve cv(ws, ws_bytes);
+  std::vector<TcPlan> plans(n > 0 ? n : 1);
+  TcDev *entries;
+  int *offsets;
+  carve_batch(cv, probs, n, plans.data(), &entries, &offsets);
+  FM_TRY(carve_ok(cv, who));
+  std::vector<TcDev> host(tc_n_entries(probs, n) + 1);
+  int ne = 0;
+  for (int i = 0; i < n; ++i) {
+    const int k = tc_prepare(&probs[i], plans[i], tune, host.data() + ne, st, who);
+    if (k < 0) return k;
+    ne += k;
+  }
+  if (ne == 0) return FM_OK;
+  int acc_cols = 32;
+  size_t smem = 0;
+  for (int e = 0; e < ne; ++e) {
+    int NT, ac;
+    tc_shape(host[e].Qt, host[e].VG, NT, ac);
+    if (ac > acc_cols) acc_cols = ac;
+    const size_t sm = tc_smem_layout(NT, host[e].VG, host[e].Qt).total;
+    if (sm > smem) smem = sm;
+  }
+  FM_REQUIRE(smem <= 232448, FM_ERR_UNSUPPORTED, "%s: tile needs %zu bytes of shared memory", who, smem);
+  for (int e0 = 0; e0 < ne; e0 += kTcEntriesPerWrite) {
+    TcEntryChunk c;
+    c.n = (ne - e0) < kTcEntriesPerWrite ? (ne - e0) : kTcEntriesPerWrite;
+    for (int k = 0; k < c.n; ++k) c.e[k] = host[e0 + k];
+    tc_write_entries_kernel<<<1, 256, 0, st>>>(c, entries + e0);
+    count_launch();
+    FM_TRY(check_launch("tc_write_entries_kernel"));
+  }
+  tc_batch_plan_kernel<<<1, 32, 0, st>>>(entries, ne, offsets);
+  count_launch();
+  FM_TRY(check_launch("tc_batch_plan_kernel"));
+  TcBatchDev B;
+  B.entries = entries;
+  B.offsets = offsets;
+  B.n_entries = ne;
+  B.acc_cols = acc_cols;
+  {
+    ScopedTimer timer(ctx, "signal_tc");
+    FM_CUDA(cudaFuncSetAttribute(signal_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    signal_tc_kernel<<<kSmCount, kTcThreads, smem, st>>>(B);
+    count_launch();
+    FM_TRY(check_launch("signal_tc_kernel"));
+  }
+  for (int i = 0; i < n; ++i) {
+    const fm_signal_args *a = &probs[i];
+    const int64_t count = a->n_ro * a->n_lines * a->n_kz * a->n_vencs;
+    if (count == 0 || a->n_nodes == 0) continue;
+    tc_reduce_kernel<<<(unsigned)ceil_div(count, 256), 256, 0, st>>>(plans[i].partials, plans[i].plan, count,
+                                                                      static_cast<float2 *>(a->out));
     count_launch();
     FM_TRY(check_launch("tc_reduce_kernel"));
   }
   return FM_OK;
 }
 
-int signal_tc_errors(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
-  Carve cv(ws, ws_bytes);
-  TcPlan pl;
-  carve_tc(cv, a, pl);
-  FM_TRY(carve_ok(cv, "fm_signal(BF16X3)"));
-  return report_errors(pl.runs, ctx->stream, "fm_signal(BF16X3)");
+int signal_tc(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
+  return tc_batch(ctx, a, 1, nullptr, ws, ws_bytes, "fm_signal(BF16X3)");
 }
+
+static int tc_batch_errors(fm_ctx *ctx, const fm_signal_args *probs, int n, void *ws, size_t ws_bytes,
+                           const char *who) {
+  Carve cv(ws, ws_bytes);
+  std::vector<TcPlan> plans(n > 0 ? n : 1);
+  TcDev *entries;
+  int *offsets;
+  carve_batch(cv, probs, n, plans.data(), &entries, &offsets);
+  FM_TRY(carve_ok(cv, who));
+  int rc = FM_OK;
+  for (int i = 0; i < n; ++i) {
+    const fm_signal_args *a = &probs[i];
+    if (a->n_ro * a->n_lines * a->n_kz == 0 || a->n_vencs == 0 || a->n_nodes == 0) continue;
+    const int r = report_errors(plans[i].runs, ctx->stream, who);
+    if (r != FM_OK && rc == FM_OK) rc = r;
+  }
+  if (n == 0) FM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return rc;
+}
+
+int signal_tc_errors(fm_ctx *ctx, const fm_signal_args *a, void *ws, size_t ws_bytes) {
+  return tc_batch_errors(ctx, a, 1, ws, ws_bytes, "fm_signal(BF16X3)");
+}
+
+int signal_tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc_tuning *tune, void *ws,
+                    size_t ws_bytes) {
+  return tc_batch(ctx, probs, n, tune, ws, ws_bytes, "fm_signal_batch");
+}
+
+int signal_tc_batch_errors(fm_ctx *ctx, const fm_signal_args *probs, int n, void *ws, size_t ws_bytes) {
+  return tc_batch_errors(ctx, probs, n, ws, ws_bytes, "fm_signal_batch");
+}
+
+size_t tc_batch_workspace_size(const fm_signal_args *probs, int n) { return tc_batch_workspace(probs, n); }
 
 }  // namespace fm

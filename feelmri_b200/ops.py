@@ -250,6 +250,75 @@ def signal(inp: SignalInputs, motion: LoweredMotion, precision: str = "f32",
     return out
 
 
+@dataclass(frozen=True)
+class Tuning:
+    """Work-unit shape of the batched tensor-core Signal (fm_tc_tuning):
+    nodes per unit (0: spread each problem over the SMs) and the most kz
+    values per tile (0: up to 64)."""
+    split_nodes: int = 0
+    kz_cap: int = 0
+
+    def struct(self) -> L.TcTuning:
+        t = L.TcTuning()
+        t.split_nodes, t.kz_cap = int(self.split_nodes), int(self.kz_cap)
+        return t
+
+
+class SignalBatch:
+    """n split-BF16 Signal problems contracted by one persistent tensor-core
+    launch.  Holds the argument array, the lowered motions and the workspace,
+    so a batch can be enqueued repeatedly (for instance inside a CUDA graph
+    capture) with the same buffers."""
+
+    def __init__(self, problems: list[tuple[SignalInputs, LoweredMotion, torch.Tensor]],
+                 tuning: Tuning | None = None):
+        if not problems:
+            raise ValueError("empty batch")
+        self.dev = problems[0][0].r0.device
+        self.problems = problems  # keeps the motion descriptors alive
+        self.tuning = tuning or Tuning()
+        self._tune = self.tuning.struct()
+        self.args = (L.SignalArgs * len(problems))()
+        for i, (inp, motion, out) in enumerate(problems):
+            if inp.r0.device != self.dev:
+                raise ValueError("all problems of a batch must be on one device")
+            self.args[i] = signal_args(inp, motion, "bf16x3", out)
+        nbytes = C.c_size_t()
+        L.check(L.lib().fm_signal_batch_workspace_size(self.args, len(problems), C.byref(nbytes)))
+        self.ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=self.dev)
+
+    @property
+    def outs(self) -> list[torch.Tensor]:
+        return [o for _, _, o in self.problems]
+
+    def enqueue(self) -> None:
+        """Queues the batch on the current stream (no host wait)."""
+        L.check(L.lib().fm_signal_batch_enqueue(ctx_for(self.dev), self.args, len(self.problems),
+                                                C.byref(self._tune), self.ws.data_ptr(), self.ws.numel()))
+
+    def status(self) -> None:
+        """Waits for the stream and raises the errors the device work found."""
+        L.check(L.lib().fm_signal_batch_status(ctx_for(self.dev), self.args, len(self.problems),
+                                               self.ws.data_ptr(), self.ws.numel()))
+
+    def run(self) -> list[torch.Tensor]:
+        self.enqueue()
+        self.status()
+        return self.outs
+
+
+def signal_batch(problems: list[tuple[SignalInputs, LoweredMotion, torch.Tensor | None]],
+                 tuning: Tuning | None = None) -> list[torch.Tensor]:
+    """Split-BF16 k-spaces of several problems (each (inputs, motion, out or
+    None)) from one persistent tensor-core launch."""
+    full = []
+    for inp, motion, out in problems:
+        if out is None:
+            out = torch.empty((*inp.kx.shape, inp.Mxy.shape[1]), dtype=torch.complex64, device=inp.r0.device)
+        full.append((inp, motion, out))
+    return SignalBatch(full, tuning).run()
+
+
 def signal_workspace_bytes(a: L.SignalArgs, precision: str) -> int:
     nbytes = C.c_size_t()
     L.check(L.lib().fm_signal_workspace_size(C.byref(a), PRECISIONS[precision], C.byref(nbytes)))

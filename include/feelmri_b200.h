@@ -258,6 +258,29 @@ FM_API int fm_signal_status(fm_ctx *ctx, const fm_signal_args *args, int precisi
                             void *workspace, size_t workspace_bytes);
 FM_API int fm_signal_workspace_size(const fm_signal_args *args, int precision,
                              size_t *bytes);
+/* Batched split-BF16 Signal (no counterpart in the reference, which calls
+ * Signal once per phantom, e.g. examples/phase_contrast.py:207): n problems,
+ * each an fm_signal_args with its own mesh, trajectory, columns, motion and
+ * output (float inputs, as FM_PREC_BF16X3), prepared one after another and
+ * then contracted by ONE persistent tensor-core launch over the work units
+ * of all of them.  Enqueue-only (capturable in a CUDA graph); the status
+ * call waits and reports device errors.  A problem's result depends on the
+ * problem and the tuning only, not on the rest of the batch.  `tune` may be
+ * NULL (defaults). */
+typedef struct fm_tc_tuning {
+  int32_t split_nodes;  /* nodes per unit along the node range (0: spread one
+                           problem's units evenly over the SMs)             */
+  int32_t kz_cap;       /* most kz values per tile of a factored run (0: up
+                           to 64 within 128 (kz, column) pairs)             */
+  int32_t reserved[2];
+} fm_tc_tuning;
+
+FM_API int fm_signal_batch_workspace_size(const fm_signal_args *probs, int n_probs, size_t *bytes);
+FM_API int fm_signal_batch_enqueue(fm_ctx *ctx, const fm_signal_args *probs, int n_probs,
+                                   const fm_tc_tuning *tune, void *workspace, size_t workspace_bytes);
+FM_API int fm_signal_batch_status(fm_ctx *ctx, const fm_signal_args *probs, int n_probs,
+                                  void *workspace, size_t workspace_bytes);
+
 /* Number of distinct-time runs of t (MRI.cpp:109-134 refreshes positions,
  * off-resonance and decay once per run).  `t` is a HOST array here. */
 FM_API int64_t fm_signal_count_time_runs(const void *t_host, int64_t n_samples,

@@ -59,6 +59,7 @@ STRUCTS = {
                                     "final_stride"]),
     "fm_signal_args": (L.SignalArgs, ["n_nodes", "m_nnz", "m_data", "kx", "Mxy", "motion", "out"]),
     "fm_mass_args": (L.MassArgs, ["n_elems", "nodes_per_elem", "elems", "n_qpoints", "tabulated"]),
+    "fm_tc_tuning": (L.TcTuning, ["split_nodes", "kz_cap", "reserved"]),
 }
 
 
