@@ -143,6 +143,30 @@ def hard_pulse_block(t0, flip_deg, tr, rf_dur=0.1, dt_rf=0.01, dt=0.1, grad=None
     return Block(times, rf, G, store_magnetization=store)
 
 
+def spamm_block(t0, tag_spacing=0.008, axis=0, rf_dur=0.1, dt_rf=0.01, lobe=0.5, dt=0.01, tail=1.0) -> Block:
+    """SPAMM tagging as examples/spamm.py:116-125 builds it: a 90-degree hard
+    pulse, a gradient lobe along `axis` of area ke / gamma with
+    ke = 2 pi / tag_spacing (785.4 rad/m at 8 mm), a second 90-degree hard
+    pulse (same phase), then free precession for `tail` ms; Mz is left
+    modulated as -cos(ke x)."""
+    n_rf = int(round(rf_dur / dt_rf))
+    ke = 2.0 * np.pi / tag_spacing
+    g = ke / (GAMMA * lobe)  # mT/m
+    t_rf1 = t0 + dt_rf * np.arange(n_rf + 1)
+    t_lobe = t_rf1[-1] + dt * np.arange(1, int(round(lobe / dt)) + 1)
+    t_rf2 = t_lobe[-1] + dt_rf * np.arange(1, n_rf + 1)
+    t_tail = t_rf2[-1] + 0.1 * np.arange(1, int(round(tail / 0.1)) + 1)
+    times = np.concatenate([t_rf1, t_lobe, t_rf2, t_tail])
+    amp = np.deg2rad(90.0) / (GAMMA * rf_dur)
+    rf = np.zeros(times.size, np.complex64)
+    rf[1:n_rf + 1] = amp
+    i2 = n_rf + 1 + t_lobe.size
+    rf[i2:i2 + n_rf] = amp
+    G = np.zeros((times.size, 3), np.float32)
+    G[n_rf + 1:n_rf + 1 + t_lobe.size, axis] = g
+    return Block(times, rf, G)
+
+
 def spoiled_gre(n_pulses=20, flip_deg=15.0, tr=5.0) -> list[Block]:
     return [hard_pulse_block(i * tr, flip_deg, tr, store=(i == n_pulses - 1)) for i in range(n_pulses)]
 
