@@ -64,18 +64,22 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, period_ms: int = 50):
         self.idx = device_index
+        self.period_ms = period_ms
         self.proc = None
         self.lines: list[str] = []
+        self._first = threading.Event()
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the timed region starts once samples flow
+            self._first.wait(timeout=10.0)
         except OSError:
             self.proc = None
         return self
@@ -83,6 +87,7 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self._first.set()
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -239,7 +244,12 @@ def run_gpu(args) -> dict | None:
             roof = {"bound": "tensor", "achieved": flops / k_avg_s / 1e12, "peak": peaks["bf16_tflops"],
                     "unit": "TFLOP/s"}
         roof["frac"] = roof["achieved"] / roof["peak"]
-        roof["traffic"] = None
+        # DRAM bytes of one full-size launch of the dominant kernel, from one ncu
+        # capture (dram__bytes_read.sum + dram__bytes_write.sum, a one-pass metric
+        # pair) of this command: 16.48 MB read + 0.03 MB written.  The node data is
+        # read from DRAM about once and reused from L2 by the work units.
+        roof["traffic"] = 16.51e6 if precision == "bf16x3" and N == 200740 else None
+        roof["traffic_unit"] = "bytes per launch"
         roof["kernel"] = kname
         roof["kernel_ms"] = k_ms / max(k_n, 1)
         roof["peak_source"] = "measured" if "note" not in peaks else "fallback"
@@ -547,6 +557,83 @@ def run_batching(args) -> dict:
     }
 
 
+# -------------------------------------------------------- serving (cfg 4) --
+
+def build_serving_requests(n_requests: int, rate: float, seed: int = 5, max_nodes: int = 200_000,
+                           max_samples: int = 262_144, max_frames: int = 4):
+    """A Poisson request stream: meshes log-uniform in [10k, max_nodes] nodes,
+    T1/T2 as in the plain configuration, Cartesian / radial / stack-of-spirals
+    trajectories of 16k-max_samples samples, 1-8 coils, 1-max_frames frames
+    with sinusoidal POD motion (rank 3) on every other request."""
+    from feelmri_b200 import workloads as W
+    from feelmri_b200.serving import Request
+    rng = np.random.default_rng(seed)
+    shapes = (W.cylinder, W.ellipsoid, W.tube)
+    t = 0.0
+    reqs = []
+    for i in range(n_requests):
+        t += rng.exponential(1.0 / rate)
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(max_nodes))))
+        mesh = shapes[i % 3](n)
+        N = mesh.n_nodes
+        S = np.exp(rng.uniform(np.log(16384), np.log(max_samples)))
+        kind = i % 3
+        if kind == 0:
+            n_kz = 16
+            side = max(8, int(round(np.sqrt(S / n_kz))))
+            traj = W.cartesian(res=(side, side, n_kz))
+        elif kind == 1:
+            n_sp = 512
+            traj = W.radial3d(n_ro=max(8, int(round(S / n_sp))), n_spokes=n_sp, kmax=500.0)
+        else:
+            il, n_kz = 16, 16
+            traj = W.spiral_stack(n_ro=max(16, int(round(S / (il * n_kz)))), n_interleaves=il, n_kz=n_kz)
+        T1, T2 = W.tissue(N, seed + i)
+        coils = W.coil_maps(mesh.nodes, int(rng.integers(1, 9)), seed=seed + i)
+        pod = W.sinusoidal_pod(N, n_modes=3, amp=1e-3, period=800.0, n_frames=8, seed=seed + i) if i % 2 else None
+        blocks = [W.hard_pulse_block(0.0, 15.0, 5.0, grad=((2.0, 0.0, 0.0), 1.0, 1.0)),
+                  W.hard_pulse_block(5.0, 15.0, 5.0)]
+        reqs.append(Request(rid=i, mesh=mesh, T1=T1, T2=T2, phi=W.off_resonance(N, 20.0, seed + i), blocks=blocks,
+                            traj=traj, coils=coils, frames=int(rng.integers(1, max_frames + 1)), pod=pod,
+                            arrival=t))
+    return reqs
+
+
+def run_serving(args) -> dict:
+    """Requests arrive as a Poisson stream and are served continuously: each
+    admitted request keeps its mesh, tissue, mass weights and magnetisation on
+    the device and runs its frames on its own stream; requests are admitted as
+    slots and HBM free up.  Reports latency percentiles and throughput."""
+    import torch
+    from feelmri_b200.serving import Server
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    t0 = time.perf_counter()
+    reqs = build_serving_requests(args.requests, args.rate)
+    build_s = time.perf_counter() - t0
+    # warm-up: one small request through a server (kernels loaded, contexts made)
+    Server(device=dev, slots=1).serve(build_serving_requests(1, args.rate, seed=99, max_nodes=12_000,
+                                                             max_samples=20_000, max_frames=1), realtime=False)
+    srv = Server(device=dev, slots=args.slots)
+    t0 = time.perf_counter()
+    items = srv.serve(reqs, realtime=True)
+    wall = time.perf_counter() - t0
+    stats = Server.summary(items)
+    work = sum(it.req.work for it in items if it.error is None)
+    return {
+        "metric": METRIC, "value": work / wall, "unit": "node*k-sample/s", "n_gpus": 1, "steps": 1,
+        "warmup": 1, "ms_per_step": wall * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic (seeded request stream)",
+        "config": {"workload": f"serving: {len(reqs)} requests, Poisson arrivals at {args.rate} req/s, meshes "
+                               "10k-200k nodes, Cartesian / radial / stack-of-spirals 16k-262k samples, 1-8 coils, "
+                               "1-4 frames, POD motion on every other request",
+                   "slots": args.slots, "node_samples": work},
+        "latency_s": {k: stats[k] for k in ("p50_s", "p99_s", "mean_s", "max_s")},
+        "requests": stats["requests"], "failed": stats["failed"],
+        "setup_s": {"requests": build_s},
+    }
+
+
 def _lib_launches() -> int:
     from feelmri_b200 import _lib
     return _lib.launch_count()
@@ -562,8 +649,12 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--workload", default="phase_contrast", choices=["phase_contrast", "batching"],
-                    help="phase_contrast: the metric's configuration; batching: many phantoms in one launch")
+    ap.add_argument("--workload", default="phase_contrast", choices=["phase_contrast", "batching", "serving"],
+                    help="phase_contrast: the metric's configuration; batching: many phantoms in one launch; "
+                         "serving: a Poisson request stream")
+    ap.add_argument("--requests", type=int, default=24)
+    ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--phantoms", type=int, default=BATCH_PHANTOMS)
     ap.add_argument("--nodes", type=int, default=N_NODES,
                     help="mesh size (smaller cases of the same workload for profiling; the metric uses the default)")
@@ -572,6 +663,8 @@ def main():
         res = run_reference(args)
     elif args.workload == "batching":
         res = run_batching(args)
+    elif args.workload == "serving":
+        res = run_serving(args)
     else:
         res = run_gpu(args)
     if res is not None:
