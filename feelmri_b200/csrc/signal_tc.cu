@@ -60,8 +60,12 @@ constexpr uint32_t kAStageBytes = kTcRows * 2 * kTcNodes * 2;  // 128 rows x 32 
 struct TcRun {
   int start, P, Q, factored;
 };
+// A work item: rows p0.. and columns q0.. of run `run`, or (nrun > 1) the
+// whole slabs of runs run .. run + nrun - 1 stacked block-diagonally: rows
+// r P + p and column pairs r Q VG + j belong to run `run + r`, and only the
+// diagonal blocks of the product are read.
 struct TcItem {
-  int run, p0, q0;
+  int run, p0, q0, nrun;
 };
 
 struct TcDev {
@@ -78,6 +82,7 @@ struct TcDev {
   const TcRun *runs;
   const TcItem *items;
   int Qt, NT, kind;  // kind 0: factored runs, 1: generic runs
+  int wrows;         // weight rows per node buffer: VG, or (stacked runs) nrun VG
   const int *plan;  // device: [2] factored items, [3] generic items, [4] splits, [5] nodes per split
   float2 *partials; // (splits, S, V) when splits > 1
   float2 *out;
@@ -129,6 +134,7 @@ struct TcSmem {
 
 // Node data is double-buffered: block b is read while block b + 1 is written.
 __host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
+  // VG here is the weight rows per node buffer (TcDev::wrows)
   TcSmem L;
   L.a_hi = 0;
   L.a_lo = kAStageBytes;
@@ -182,8 +188,9 @@ __device__ inline void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint3
 
 struct TcUnit {
   TcItem it;
-  TcRun run;
+  TcRun run;  // the first run
   int split, P_tile, Q_tile, n_stages, n_groups;
+  int rows, pairs;  // active A rows (nrun P_tile) and column pairs (nrun Q_tile VG)
   int64_t n_begin, n_end;
 };
 
@@ -195,6 +202,8 @@ __device__ inline TcUnit tc_unit(const TcDev &p, const TcWork &W, int u) {
   U.run = p.runs[U.it.run];
   U.P_tile = min(kTcRows, U.run.P - U.it.p0);
   U.Q_tile = min(p.Qt, U.run.Q - U.it.q0);
+  U.rows = U.it.nrun * U.P_tile;
+  U.pairs = U.it.nrun * U.Q_tile * p.VG;
   U.n_begin = (int64_t)U.split * W.chunk;
   U.n_end = min(p.N, U.n_begin + W.chunk);
   U.n_stages = U.n_end > U.n_begin ? (int)ceil_div(U.n_end - U.n_begin, kTcNodes) : 0;
@@ -246,7 +255,7 @@ __device__ inline void tc_load_raw(const TcDev &p, int64_t n, TcRaw &r) {
 // off-resonance rotated weights W' = (M Mxy)[n, v] exp(-t / T2) exp(i phi t).
 // Nodes past the range get position 0 and zero weights, so they add nothing.
 __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, const TcRaw &r, const float *wrun,
-                                 float tg, double *pos, float2 *wblk, int slot) {
+                                 double *pos, float2 *wblk, int slot) {
   if (n < U.n_end) {
     float x = r.x, y = r.y, z = r.z;
     if (p.md.kind == FM_MOTION_TERMS) {
@@ -260,19 +269,24 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
     pos[slot] = (double)x;
     pos[kTcBlockNodes + slot] = (double)y;
     pos[2 * kTcBlockNodes + slot] = (double)z;
-    const float decay = expf(-tg * (1.0f / r.t2));
-    float so, co;
-    sincosf(r.phi * tg, &so, &co);
-    const float er = decay * co, ei = decay * so;
+    // one weight set per run of the unit (stacked runs share positions)
+    for (int k = 0; k < U.it.nrun; ++k) {
+      const float tg = (float)p.run_t[U.it.run + k];
+      const float decay = expf(-tg * (1.0f / r.t2));
+      float so, co;
+      sincosf(r.phi * tg, &so, &co);
+      const float er = decay * co, ei = decay * so;
+      float2 *wk = wblk + k * p.VG * kWStride;
 #pragma unroll
-    for (int v = 0; v < kTcVGroup; ++v)
-      if (v < p.VG)
-        wblk[v * kWStride + slot] = make_float2(r.m[v].x * er - r.m[v].y * ei, r.m[v].x * ei + r.m[v].y * er);
+      for (int v = 0; v < kTcVGroup; ++v)
+        if (v < p.VG)
+          wk[v * kWStride + slot] = make_float2(r.m[v].x * er - r.m[v].y * ei, r.m[v].x * ei + r.m[v].y * er);
+    }
   } else {
     pos[slot] = 0.0;
     pos[kTcBlockNodes + slot] = 0.0;
     pos[2 * kTcBlockNodes + slot] = 0.0;
-    for (int v = 0; v < p.VG; ++v) wblk[v * kWStride + slot] = make_float2(0.f, 0.f);
+    for (int v = 0; v < U.it.nrun * p.VG; ++v) wblk[v * kWStride + slot] = make_float2(0.f, 0.f);
   }
 }
 
@@ -340,9 +354,13 @@ __device__ inline void tc_final(const TcDev &p, int acc_cols, const TcWork &W, c
   const int quarter = warp & 3;
   const int row = quarter * 32 + (tid & 31);
   const int NH = p.NT >> 1;
-  const bool row_ok = row < U.P_tile;
+  const bool row_ok = row < U.rows;
   float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
-  const int s_row = U.run.start + (U.run.factored ? (U.it.p0 + row) * p.n_kz + U.it.q0 : U.it.p0 + row);
+  // row r P_tile + pl belongs to run `run + r`; only that run's column block is read
+  const int r_row = row_ok ? row / U.P_tile : 0, pl = row_ok ? row % U.P_tile : 0;
+  const int qvg = U.Q_tile * p.VG;
+  const int start = row_ok ? p.runs[U.it.run + r_row].start : 0;
+  const int s_row = start + (U.run.factored ? (U.it.p0 + pl) * p.n_kz + U.it.q0 : U.it.p0 + pl);
   const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
   for (int c0 = (warp >> 2) * 8; c0 < NH; c0 += 32) {
     uint32_t r[8], m[8], sr[8], sm[8];
@@ -361,8 +379,10 @@ __device__ inline void tc_final(const TcDev &p, int acc_cols, const TcWork &W, c
         re = __uint_as_float(sr[i]) + re;
         im = __uint_as_float(sm[i]) + im;
       }
-      const int jj = c0 + i;  // pair (q, v)
-      const int q = jj / p.VG, vv = jj % p.VG;
+      const int jj = c0 + i;  // pair (run block, q, v)
+      if (jj / qvg != r_row) continue;
+      const int jv = jj % qvg;
+      const int q = jv / p.VG, vv = jv % p.VG;
       if (q < U.Q_tile) dst[(int64_t)(s_row + q) * p.V + p.v0 + vv] = make_float2(re, im);
     }
   }
@@ -449,8 +469,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     }
     const TcDev &p = B.entries[e_lo];
     const TcWork W = tc_work(p);
-    const int NT = p.NT, NH = NT >> 1, VG = p.VG, Qt = p.Qt;
-    const TcSmem L = tc_smem_layout(NT, VG, Qt);
+    const int NT = p.NT, NH = NT >> 1, VG = p.VG, Qt = p.Qt, WR = p.wrows;
+    const TcSmem L = tc_smem_layout(NT, WR, Qt);
     double *pos_all = reinterpret_cast<double *>(smem + L.pos);
     float2 *w_all = reinterpret_cast<float2 *>(smem + L.w);
     float2 *etab = reinterpret_cast<float2 *>(smem + L.etab);
@@ -470,18 +490,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     ptx::named_barrier(1, kTcProducers);  // the previous unit's readers are done
     // per-unit row data in registers
     double kx0 = 0, ky0 = 0, kz0 = 0, kx1 = 0, ky1 = 0, kz1 = 0;  // A: kp of the row; B: kq of q and q + 32
-    int bq = 0, bv = 0;
+    int bq = 0, bw = 0;  // B: phase-table row and weight row of the pair
     if (a_role) {
-      if (row < U.P_tile) {
-        const int s_p = U.run.start + (fac ? (U.it.p0 + row) * p.n_kz : U.it.p0 + row);
+      if (row < U.rows) {
+        // row r P_tile + pl belongs to run `run + r` (r = 0 unless stacked)
+        const int r = row / U.P_tile, pl = row % U.P_tile;
+        const int start = r == 0 ? U.run.start : p.runs[U.it.run + r].start;
+        const int s_p = start + (fac ? (U.it.p0 + pl) * p.n_kz : U.it.p0 + pl);
         kx0 = p.kx[s_p];
         ky0 = p.ky[s_p];
         kz0 = p.kz[s_p];
       }
     } else {
-      if (row < U.Q_tile * VG) {
-        bq = row / VG;
-        bv = row % VG;
+      if (row < U.pairs) {
+        const int qvg = U.Q_tile * VG;
+        const int r = row / qvg, jv = row % qvg;
+        bq = jv / VG;
+        bw = r * VG + jv % VG;
       }
       if (fac) {
         const int s_0 = U.run.start;
@@ -501,13 +526,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     }
     const bool t_on0 = !a_role && fac && tq < U.Q_tile, t_on1 = !a_role && fac && tq + 32 < U.Q_tile;
     const float *wrun = p.weights ? p.weights + (int64_t)U.it.run * p.md.slots : nullptr;
-    const float tg = (float)p.run_t[U.it.run];
     const uint32_t n_blocks = (nst + kTcStagesPerBlock - 1) / kTcStagesPerBlock;
     // prologue: node block 0 into buffer 0
     if (loader && nst > 0) {
       const int64_t n = U.n_begin + tid;
       if (n < U.n_end) tc_load_raw(p, n, raw);
-      tc_derive(p, U, n, raw, wrun, tg, pos_all, w_all, tid);
+      tc_derive(p, U, n, raw, wrun, pos_all, w_all, tid);
     }
     ptx::named_barrier(1, kTcProducers);  // block 0 is visible
     if (nst > 0) {
@@ -545,8 +569,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           if (j == 4) {
             if (n1 < U.n_end) tc_load_raw(p, n1, raw);
           } else {
-            tc_derive(p, U, n1, raw, wrun, tg, pos_all + (buf ^ 1) * 3 * kTcBlockNodes,
-                      w_all + (buf ^ 1) * VG * kWStride, tid);
+            tc_derive(p, U, n1, raw, wrun, pos_all + (buf ^ 1) * 3 * kTcBlockNodes,
+                      w_all + (buf ^ 1) * WR * kWStride, tid);
           }
         }
         tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
@@ -572,7 +596,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           st_shared_v4(stg + gl0, l[0], l[1], l[2], l[3]);
         }
         if (g_b) {
-          const float2 wv = w_all[(buf * VG + gv) * kWStride + j * kTcNodes + gnode];
+          const float2 wv = w_all[(buf * WR + gv) * kWStride + j * kTcNodes + gnode];
           uint32_t hb, lb;
           split_pair(wv.x, wv.y, hb, lb);
           const uint32_t hm = __byte_perm(hb, 0u, 0x1032) ^ 0x80000000u, lm = __byte_perm(lb, 0u, 0x1032) ^ 0x80000000u;
@@ -589,7 +613,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       }
     } else if (a_role) {
       // ------------------------------------------------------- A rows --
-      const bool active = (rw >> 1) * 32 < U.P_tile;
+      const bool active = (rw >> 1) * 32 < U.rows;
       for (uint32_t st = 0; st < nst; ++st) {
         const uint32_t g = g0 + st, s = g & (kTcStages - 1);
         const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
@@ -601,8 +625,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           if (j == 4) {
             if (n1 < U.n_end) tc_load_raw(p, n1, raw);
           } else {
-            tc_derive(p, U, n1, raw, wrun, tg, pos_all + (buf ^ 1) * 3 * kTcBlockNodes,
-                      w_all + (buf ^ 1) * VG * kWStride, tid);
+            tc_derive(p, U, n1, raw, wrun, pos_all + (buf ^ 1) * 3 * kTcBlockNodes,
+                      w_all + (buf ^ 1) * WR * kWStride, tid);
           }
         }
         // wait until the MMAs that last read stage s are done
@@ -654,7 +678,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         // B'^T rows: re row `row` = (Re B, Im B), im row NT/2 + row =
         // (Im B, -Re B), B = e_q(n) W'(n, v).  Pairs past Q_tile VG hold
         // values no output reads.
-        const float4 *wp = reinterpret_cast<const float4 *>(w_all + (buf * VG + bv) * kWStride + j * kTcNodes + 8 * half);
+        const float4 *wp = reinterpret_cast<const float4 *>(w_all + (buf * WR + bw) * kWStride + j * kTcNodes + 8 * half);
         float br[8], bi[8];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -716,10 +740,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, gst - 1, nst - 1, nst);
     }
     if (U.n_groups > 0) tc_final(p, B.acc_cols, W, U, accfull, tmem, gbase + U.n_groups - 1, U.n_groups > 1, abort_flag);
-    if (U.n_groups == 0 && tid < kTcRows && tid < U.P_tile) {
+    if (U.n_groups == 0 && tid < U.rows) {
       // no nodes in this split: its share of the tile is zero
       float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
-      const int s_row = U.run.start + (fac ? (U.it.p0 + tid) * p.n_kz + U.it.q0 : U.it.p0 + tid);
+      const int r = tid / U.P_tile, pl = tid % U.P_tile;
+      const int start = p.runs[U.it.run + r].start;
+      const int s_row = start + (fac ? (U.it.p0 + pl) * p.n_kz + U.it.q0 : U.it.p0 + pl);
       for (int q = 0; q < U.Q_tile; ++q)
         for (int v = 0; v < VG; ++v) dst[(int64_t)(s_row + q) * p.V + p.v0 + v] = make_float2(0.f, 0.f);
     }
@@ -781,14 +807,48 @@ __global__ void tc_classify_kernel(const float *__restrict__ kx, const float *__
   }  // runs
 }
 
+// Runs can be stacked into one unit when the positions do not depend on the
+// run (no motion) and every run is a factored slab of the full (lines x kz)
+// shape with the same kz offsets kq = k(q) - k(first sample), exactly.
+// `flag` starts non-zero; any run that breaks a condition clears it.
+__global__ void tc_stack_check_kernel(const float *__restrict__ kx, const float *__restrict__ ky,
+                                      const float *__restrict__ kz, const TcRun *__restrict__ runs,
+                                      const int *__restrict__ counts, int n_lines, int n_kz, int *__restrict__ flag) {
+  const int n_runs = counts[0];
+  if (n_runs <= 0) return;
+  const int s0 = runs[0].start;
+  const int64_t total = (int64_t)n_runs * n_kz;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int g = (int)(idx / n_kz), q = (int)(idx % n_kz);
+    const TcRun r = runs[g];
+    bool ok = r.factored && r.P == n_lines && r.Q == n_kz;
+    if (ok) {
+      const int a = r.start, b = s0;
+      ok = ((double)kx[a + q] - (double)kx[a]) == ((double)kx[b + q] - (double)kx[b]) &&
+           ((double)ky[a + q] - (double)ky[a]) == ((double)ky[b + q] - (double)ky[b]) &&
+           ((double)kz[a + q] - (double)kz[a]) == ((double)kz[b + q] - (double)kz[b]);
+    }
+    if (!ok) atomicExch(flag, 0);
+  }
+}
+
 // Item counts per run, factored runs in one list and the rest in another.
+// With stacking (stack != nullptr and *stack set), every R-th run opens one
+// item of up to R runs.
 __global__ void tc_count_kernel(const TcRun *__restrict__ runs, const int *__restrict__ counts, int Qt,
-                                int *__restrict__ nf, int *__restrict__ ng, int64_t S) {
+                                int *__restrict__ nf, int *__restrict__ ng, int64_t S, const int *__restrict__ stack,
+                                int R) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = counts[0];
   if (g > S) return;
   if (g >= n) {
     nf[g] = 0;
+    ng[g] = 0;
+    return;
+  }
+  if (stack && *stack && R > 1) {
+    nf[g] = (g % R == 0) ? 1 : 0;
     ng[g] = 0;
     return;
   }
@@ -802,13 +862,24 @@ __global__ void tc_count_kernel(const TcRun *__restrict__ runs, const int *__res
 // go to plan[2] and plan[3].
 __global__ void tc_fill_kernel(const TcRun *__restrict__ runs, const int *__restrict__ counts, int Qt,
                                const int *__restrict__ of, const int *__restrict__ og, TcItem *__restrict__ items,
-                               int *__restrict__ plan) {
+                               int *__restrict__ plan, const int *__restrict__ stack, int R) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = counts[0];
   if (g > n) return;
   if (g == n) {
     plan[2] = of[n];
     plan[3] = og[n];
+    return;
+  }
+  if (stack && *stack && R > 1) {
+    if (g % R == 0) {
+      TcItem t;
+      t.run = g;
+      t.p0 = 0;
+      t.q0 = 0;
+      t.nrun = (n - g) < R ? (n - g) : R;
+      items[of[g]] = t;
+    }
     return;
   }
   const TcRun r = runs[g];
@@ -823,6 +894,7 @@ __global__ void tc_fill_kernel(const TcRun *__restrict__ runs, const int *__rest
       t.run = g;
       t.p0 = a * kTcRows;
       t.q0 = b * qt;
+      t.nrun = 1;
       items[base + a * nq + b] = t;
     }
 }
@@ -919,6 +991,7 @@ struct TcPlan {
   TcItem *items;  // n_groups lists of 2 S + 2
   int *nf, *ng, *of, *og;
   int *plan;      // n_groups rows of 8 ints
+  int *stack;     // runs can be stacked (set on the device)
   float2 *partials;
   int n_groups, max_splits;
 };
@@ -947,6 +1020,7 @@ static void carve_tc(Carve &c, const fm_signal_args *a, TcPlan &pl) {
   pl.of = c.take<int>(S + 2);
   pl.og = c.take<int>(S + 2);
   pl.plan = c.take<int>((size_t)8 * (pl.n_groups > 0 ? pl.n_groups : 1));
+  pl.stack = c.take<int>(4);
   pl.max_splits = tc_max_splits(S, V);
   pl.partials = c.take<float2>((size_t)pl.max_splits * S * V);
 }
@@ -972,6 +1046,20 @@ static int tc_qt(const fm_signal_args *a, int VG, const fm_tc_tuning *tune) {
   int cap = (128 / VG < 64) ? 128 / VG : 64;
   if (tune && tune->kz_cap > 0 && tune->kz_cap < cap) cap = tune->kz_cap;
   return (int)((a->n_kz < cap) ? a->n_kz : cap);
+}
+
+// Runs per stacked unit for a column group: whole slabs only (lines <= 128
+// rows, kz within one tile), at most 128 rows, 128 column pairs and 8 weight
+// rows, and only without motion (the runs then share node positions).
+static int tc_stack_runs(const fm_signal_args *a, int VG, int Qt) {
+  if (a->motion && a->motion->kind != FM_MOTION_NONE) return 1;
+  if (a->n_kz < 2 || a->n_lines * a->n_kz < 2 || a->n_kz > Qt || a->n_lines > kTcRows) return 1;
+  int R = kTcRows / (int)a->n_lines;
+  const int by_pairs = kTcRows / (int)(a->n_kz * VG);
+  const int by_weights = kTcVGroup / VG;
+  if (by_pairs < R) R = by_pairs;
+  if (by_weights < R) R = by_weights;
+  return R < 2 ? 1 : R;
 }
 
 static void tc_shape(int Qt, int VG, int &NT, int &acc_cols) {
@@ -1016,15 +1104,33 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
                                                            (int)a->n_lines, (int)a->n_kz, pl.tcruns);
   count_launch();
   FM_TRY(check_launch("tc_classify_kernel"));
+  // stacking check (the same for every column group)
+  bool may_stack = false;
+  for (int g = 0; g < pl.n_groups; ++g) {
+    const int64_t v0 = (int64_t)g * kTcVGroup;
+    const int VG = (int)((V - v0) < kTcVGroup ? (V - v0) : kTcVGroup);
+    if (tc_stack_runs(a, VG, tc_qt(a, VG, tune)) > 1) may_stack = true;
+  }
+  if (may_stack) {
+    FM_CUDA(cudaMemsetAsync(pl.stack, 1, sizeof(int), st));
+    const int64_t work = S;  // n_runs x n_kz <= S
+    const unsigned blocks = (unsigned)(work / 256 + 1 < 4 * kSmCount ? work / 256 + 1 : 4 * kSmCount);
+    tc_stack_check_kernel<<<blocks, 256, 0, st>>>(kx, ky, kz, pl.tcruns, pl.runs.counts, (int)a->n_lines,
+                                                   (int)a->n_kz, pl.stack);
+    count_launch();
+    FM_TRY(check_launch("tc_stack_check_kernel"));
+  }
   int ne = 0;
   for (int g = 0; g < pl.n_groups; ++g) {
     const int64_t v0 = (int64_t)g * kTcVGroup;
     const int VG = (int)((V - v0) < kTcVGroup ? (V - v0) : kTcVGroup);
     const int Qt_f = tc_qt(a, VG, tune);
+    const int R = tc_stack_runs(a, VG, Qt_f);
+    const int *stack = R > 1 ? pl.stack : nullptr;
     TcItem *items = pl.items + (size_t)g * (2 * S + 2);
     int *plan = pl.plan + 8 * g;
     const unsigned gb = (unsigned)ceil_div(S + 1, 256);
-    tc_count_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.nf, pl.ng, S);
+    tc_count_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.nf, pl.ng, S, stack, R);
     count_launch();
     FM_TRY(check_launch("tc_count_kernel"));
     size_t cb = pl.runs.cub_bytes;
@@ -1032,7 +1138,7 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
     cb = pl.runs.cub_bytes;
     FM_CUDA(cub::DeviceScan::ExclusiveSum(pl.runs.cub_tmp, cb, pl.ng, pl.og, (int)(S + 1), st));
     count_launch(2);
-    tc_fill_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.of, pl.og, items, plan);
+    tc_fill_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.of, pl.og, items, plan, stack, R);
     count_launch();
     FM_TRY(check_launch("tc_fill_kernel"));
     for (int kind = 0; kind < 2; ++kind) {
@@ -1059,8 +1165,11 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
       p.error = pl.runs.error;
       p.kind = kind;
       p.Qt = kind == 0 ? Qt_f : 1;
+      // a stacked unit holds R runs' columns and weight rows
+      const int Rk = kind == 0 ? R : 1;
+      p.wrows = Rk * VG;
       int acc_cols;
-      tc_shape(p.Qt, VG, p.NT, acc_cols);
+      tc_shape(p.Qt, Rk * VG, p.NT, acc_cols);
     }
   }
   tc_plan_kernel<<<1, 32, 0, st>>>(pl.plan, pl.n_groups, N, pl.max_splits, tune ? tune->split_nodes : 0);
@@ -1091,10 +1200,10 @@ static int tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc
   int acc_cols = 32;
   size_t smem = 0;
   for (int e = 0; e < ne; ++e) {
-    int NT, ac;
-    tc_shape(host[e].Qt, host[e].VG, NT, ac);
+    int NT = host[e].NT, ac = 32;
+    while (ac < NT) ac <<= 1;
     if (ac > acc_cols) acc_cols = ac;
-    const size_t sm = tc_smem_layout(NT, host[e].VG, host[e].Qt).total;
+    const size_t sm = tc_smem_layout(NT, host[e].wrows, host[e].Qt).total;
     if (sm > smem) smem = sm;
   }
   FM_REQUIRE(smem <= 232448, FM_ERR_UNSUPPORTED, "%s: tile needs %zu bytes of shared memory", who, smem);

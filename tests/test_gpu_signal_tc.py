@@ -124,3 +124,28 @@ def test_deep_node_sums_stay_accurate(cuda):
     ref = _ref(M, traj, r0, phi, T2, Mxy, idx=idx)
     err = fp64.rel_l2(K.reshape(-1, 4)[idx], ref)
     assert err < 3e-5, err
+
+
+def test_stacked_small_slabs(cuda):
+    # static positions and equal kz offsets in every run: runs of 8 lines x 8 kz
+    # are stacked several per unit; each run's block must come out alone
+    mesh, N, M, Mxy, phi, T2 = _case(n=4000, V=2, seed=5)
+    traj = W.spiral_stack(n_ro=40, n_interleaves=8, n_kz=8)
+    r0 = mesh.nodes.astype(np.float32)
+    K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    err = fp64.rel_l2(K, _ref(M, traj, r0, phi, T2, Mxy))
+    assert err < TOL, err
+    K32 = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None)
+    assert fp64.rel_l2(K, K32) < TOL
+
+
+def test_unstackable_runs_fall_back(cuda):
+    # kz offsets that change from run to run: the stacking check must refuse
+    mesh, N, M, Mxy, phi, T2 = _case(n=3000, V=1, seed=6)
+    traj = W.cartesian(res=(10, 12, 8))
+    kz = traj.kz * (1.0 + 0.01 * np.arange(10, dtype=np.float32)[:, None, None])
+    traj = W.Trajectory(traj.kx, traj.ky, kz.astype(np.float32), traj.t)
+    r0 = mesh.nodes.astype(np.float32)
+    K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    err = fp64.rel_l2(K, _ref(M, traj, r0, phi, T2, Mxy))
+    assert err < TOL, err
