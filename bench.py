@@ -557,6 +557,88 @@ def run_batching(args) -> dict:
     }
 
 
+# ------------------------------------------------------ precision (cfg 2) --
+
+def run_precision(args) -> dict:
+    """Ellipsoid phantom (semi-axes 60/50/40 mm), POD motion (rank 10,
+    Phi ~ N(0, 1 mm), sinusoidal weights, 800 ms cycle), 3-D radial readout
+    (256 readout points x 4096 spokes, |k| <= 500 1/m, one distinct time per
+    readout point), 8 Gaussian receive coils; one frame per step (a
+    15-degree excitation, then the Signal of all coils).  Split-BF16 and FP32
+    forms, each against the FP64 oracle on a seeded subset of samples."""
+    import torch
+    import scipy.sparse as sp
+    from feelmri_b200 import ops
+    from feelmri_b200._motion import lower
+    from feelmri_b200.Assemble import mass_lumped
+    from feelmri_b200.FiniteElements import FiniteElement, QuadratureRule
+    from feelmri_b200.MRI import signal_call_times
+    from feelmri_b200 import workloads as W
+    from oracle import fp64
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    mesh = W.ellipsoid(args.nodes if args.nodes != N_NODES else 500_000)
+    N = mesh.n_nodes
+    traj = W.radial3d(n_ro=256, n_spokes=args.spokes, kmax=500.0)
+    S = traj.n_samples
+    C = 8
+    T1, T2 = W.tissue(N, 2)
+    phi = W.off_resonance(N, 20.0, 2)
+    coils = W.coil_maps(mesh.nodes, C, seed=3)
+    pod = W.sinusoidal_pod(N, n_modes=10, amp=1e-3, period=800.0, n_frames=20, seed=2)
+    w = mass_lumped(mesh.elems, mesh.nodes, FiniteElement(), QuadratureRule(order=2))
+    up = lambda a, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dt)  # noqa
+    r0 = up(mesh.nodes.astype(np.float32))
+    M = ops.SparseCSC((N, N), up(np.arange(N + 1, dtype=np.int32), torch.int32),
+                      up(np.arange(N, dtype=np.int32), torch.int32), up(w.astype(np.float32)))
+    # magnetisation after a 15-degree excitation, through every coil
+    m0 = np.full(N, np.sin(np.deg2rad(15.0)), np.complex64)
+    cols = up(m0[:, None] * coils, torch.complex64)
+    sig = ops.SignalInputs(M=M, kx=up(traj.kx), ky=up(traj.ky), kz=up(traj.kz), t=up(traj.t), r0=r0, phi=up(phi),
+                           T2=up(T2), Mxy=cols)
+    res = {}
+    outs = {}
+    for prec in ("bf16x3", "f32"):
+        out = torch.empty((*traj.shape, C), dtype=torch.complex64, device=dev)
+        ms = []
+        for f in range(args.warmup + args.steps):
+            pod.update_timeshift(40.0 * f)
+            mo = lower(pod, N, dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            ops.signal(sig, mo, prec, out=out)
+            b.record()
+            b.synchronize()
+            if f >= args.warmup:
+                ms.append(a.elapsed_time(b))
+        res[prec] = statistics.median(ms)
+        outs[prec] = out.cpu().numpy().reshape(S, C)
+    # FP64 oracle on a seeded subset of the last frame's samples
+    idx = np.random.default_rng(2).choice(S, args.check_samples, replace=False)
+    times = signal_call_times(traj.t)[1:]
+
+    class _RunDisp:  # displacement of run g, computed only for the runs the subset touches
+        def __getitem__(self, g):
+            return pod(float(times[g]))
+
+    disp = _RunDisp()
+    ref = fp64.signal(sp.diags(w).tocsc(), traj.kx, traj.ky, traj.kz, traj.t, mesh.nodes.astype(np.float32), phi, T2,
+                      cols.cpu().numpy(), disp=disp, pi_mode="float", sample_idx=idx)
+    units = float(N) * S
+    return {
+        "metric": METRIC, "value": units / (res["bf16x3"] / 1e3), "unit": "node*k-sample/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["bf16x3"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic (seeded phantom, motion, coils)",
+        "config": {"workload": f"precision: {N}-node ellipsoid, POD rank 10, 3-D radial 256 x {args.spokes} "
+                               f"samples (|k| <= 500 1/m), 8 coils, one frame per step",
+                   "node_samples_per_step": units, "columns": C},
+        "f32": {"ms_per_step": res["f32"], "value": units / (res["f32"] / 1e3)},
+        "rel_l2_vs_fp64": {"bf16x3": fp64.rel_l2(outs["bf16x3"][idx], ref), "f32": fp64.rel_l2(outs["f32"][idx], ref),
+                           "samples": int(args.check_samples)},
+    }
+
+
 # -------------------------------------------------------- serving (cfg 4) --
 
 def build_serving_requests(n_requests: int, rate: float, seed: int = 5, max_nodes: int = 200_000,
@@ -649,12 +731,14 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--workload", default="phase_contrast", choices=["phase_contrast", "batching", "serving"],
+    ap.add_argument("--workload", default="phase_contrast", choices=["phase_contrast", "batching", "serving", "precision"],
                     help="phase_contrast: the metric's configuration; batching: many phantoms in one launch; "
-                         "serving: a Poisson request stream")
+                         "serving: a Poisson request stream; precision: radial, 8 coils, rank-10 motion")
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--spokes", type=int, default=4096)
+    ap.add_argument("--check-samples", type=int, default=256)
     ap.add_argument("--phantoms", type=int, default=BATCH_PHANTOMS)
     ap.add_argument("--nodes", type=int, default=N_NODES,
                     help="mesh size (smaller cases of the same workload for profiling; the metric uses the default)")
@@ -665,6 +749,8 @@ def main():
         res = run_batching(args)
     elif args.workload == "serving":
         res = run_serving(args)
+    elif args.workload == "precision":
+        res = run_precision(args)
     else:
         res = run_gpu(args)
     if res is not None:
