@@ -83,6 +83,8 @@ struct TcDev {
   const TcItem *items;
   int Qt, NT, kind;  // kind 0: factored runs, 1: generic runs
   int wrows;         // weight rows per node buffer: VG, or (stacked runs) nrun VG
+  int mm_ld;         // row stride of MM (float2): this group's columns, padded to even
+  int tma;           // node blocks are staged by bulk copies (aligned inputs, room in smem)
   const int *plan;  // device: [2] factored items, [3] generic items, [4] splits, [5] nodes per split
   float2 *partials; // (splits, S, V) when splits > 1
   float2 *out;
@@ -120,6 +122,7 @@ __device__ inline TcWork tc_work(const TcDev &p) {
 // (130 and 18 complex values) so that the B producers' 16-byte reads of
 // different columns fall in different banks.
 constexpr int kWStride = kTcBlockNodes + 2;
+constexpr uint32_t kTcSmemMax = 232448;  // dynamic shared memory a block may opt in to
 constexpr int kEStride = kTcNodes + 2;
 
 // Barriers and the tensor-memory address live in the first kTcFront bytes
@@ -129,7 +132,7 @@ constexpr uint32_t kTcBars = 0, kTcMisc = 128;
 
 struct TcSmem {
   uint32_t stage_bytes, a_hi, a_lo, b_hi, b_lo;  // offsets inside a stage
-  uint32_t stages, pos, w, etab, total;
+  uint32_t stages, pos, w, etab, raw, total;
 };
 
 // Node data is double-buffered: block b is read while block b + 1 is written.
@@ -149,8 +152,14 @@ __host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
   off += 2 * VG * kWStride * 8;
   L.etab = off;  // [2][Qt][kEStride] float2, by stage parity
   off += 2 * Qt * kEStride * 8;
+  L.raw = off;  // staging of one raw node block (bulk copies), when used
   L.total = off;
   return L;
+}
+
+// Bytes of one raw node block: positions, T2, phi and the group's M Mxy rows.
+__host__ __device__ inline uint32_t tc_raw_bytes(int mm_ld) {
+  return kTcBlockNodes * (12 + 4 + 4 + 8 * mm_ld);
 }
 
 // Byte offset of element (row, k) of a K-major, no-swizzle operand tile with
@@ -230,6 +239,17 @@ struct TcRaw {
   float2 m[kTcVGroup];
 };
 
+__device__ inline void tc_prefetch_modes(const TcDev &p, int64_t n) {
+  if (p.md.kind != FM_MOTION_TERMS) return;
+  for (int k = 0; k < p.md.n_terms; ++k) {
+    const fm_motion_term &T = p.md.terms[k];
+    if (T.kind == FM_TERM_RESPIRATORY) continue;
+    const float *Phi = T.modes + (size_t)n * 3 * T.n_modes;
+    prefetch_l1(Phi);
+    prefetch_l1(Phi + 3 * T.n_modes - 1);
+  }
+}
+
 __device__ inline void tc_load_raw(const TcDev &p, int64_t n, TcRaw &r) {
   r.x = p.r0[3 * n + 0];
   r.y = p.r0[3 * n + 1];
@@ -238,16 +258,8 @@ __device__ inline void tc_load_raw(const TcDev &p, int64_t n, TcRaw &r) {
   r.phi = p.phi[n];
 #pragma unroll
   for (int v = 0; v < kTcVGroup; ++v)
-    if (v < p.VG) r.m[v] = p.MM[n * p.V + p.v0 + v];
-  if (p.md.kind == FM_MOTION_TERMS) {
-    for (int k = 0; k < p.md.n_terms; ++k) {
-      const fm_motion_term &T = p.md.terms[k];
-      if (T.kind == FM_TERM_RESPIRATORY) continue;
-      const float *Phi = T.modes + (size_t)n * 3 * T.n_modes;
-      prefetch_l1(Phi);
-      prefetch_l1(Phi + 3 * T.n_modes - 1);
-    }
-  }
+    if (v < p.VG) r.m[v] = p.MM[n * p.mm_ld + v];
+  tc_prefetch_modes(p, n);
 }
 
 // Per-run node quantities of one node into slot `slot` of a node buffer:
@@ -287,6 +299,55 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
     pos[kTcBlockNodes + slot] = 0.0;
     pos[2 * kTcBlockNodes + slot] = 0.0;
     for (int v = 0; v < U.it.nrun * p.VG; ++v) wblk[v * kWStride + slot] = make_float2(0.f, 0.f);
+  }
+}
+
+// Node block blk + 1 of a unit, at stage j of block blk (threads 0-127, one
+// node each).  j == 4: a full block with p.tma is requested by bulk copies
+// into the staging area (thread 0; completion on rawfull), any other block by
+// register loads.  j == 6: the block is derived into the other node buffer.
+// raw_seq counts the staged blocks (the rawfull phase).
+__device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, uint32_t blk, uint32_t j,
+                                      TcRaw &raw, uint32_t &raw_seq, unsigned char *staging, uint64_t *rawfull,
+                                      const float *wrun, double *pos_next, float2 *w_next,
+                                      volatile int *abort_flag) {
+  const int64_t n0 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes;
+  const int64_t n1 = n0 + tid;
+  const bool staged = p.tma && n0 + kTcBlockNodes <= U.n_end;
+  float *sr0 = reinterpret_cast<float *>(staging);
+  float *sT2 = sr0 + 3 * kTcBlockNodes;
+  float *sphi = sT2 + kTcBlockNodes;
+  float2 *sMM = reinterpret_cast<float2 *>(sphi + kTcBlockNodes);
+  if (j == 4) {
+    if (staged) {
+      if (tid == 0) {
+        // the staging area's previous readers (the last block's derive) are
+        // past this stage's barriers; order their reads before the copies
+        ptx::fence_proxy_async_smem();
+        ptx::mbar_arrive_expect_tx(rawfull, tc_raw_bytes(p.mm_ld));
+        ptx::bulk_copy_g2s(sr0, p.r0 + 3 * n0, 12 * kTcBlockNodes, rawfull);
+        ptx::bulk_copy_g2s(sT2, p.T2 + n0, 4 * kTcBlockNodes, rawfull);
+        ptx::bulk_copy_g2s(sphi, p.phi + n0, 4 * kTcBlockNodes, rawfull);
+        ptx::bulk_copy_g2s(sMM, p.MM + n0 * p.mm_ld, 8 * kTcBlockNodes * p.mm_ld, rawfull);
+      }
+      tc_prefetch_modes(p, n1);
+    } else if (n1 < U.n_end) {
+      tc_load_raw(p, n1, raw);
+    }
+  } else {
+    if (staged) {
+      tc_wait(rawfull, raw_seq & 1, abort_flag);
+      ++raw_seq;
+      raw.x = sr0[3 * tid];
+      raw.y = sr0[3 * tid + 1];
+      raw.z = sr0[3 * tid + 2];
+      raw.t2 = sT2[tid];
+      raw.phi = sphi[tid];
+#pragma unroll
+      for (int v = 0; v < kTcVGroup; ++v)
+        if (v < p.VG) raw.m[v] = sMM[tid * p.mm_ld + v];
+    }
+    tc_derive(p, U, n1, raw, wrun, pos_next, w_next, tid);
   }
 }
 
@@ -425,6 +486,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   uint64_t *empty = reinterpret_cast<uint64_t *>(smem + kTcBars);
   uint64_t *accfull = empty + kTcStages;
   uint64_t *done = accfull + 1;
+  uint64_t *rawfull = done + 1;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kTcMisc);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + kTcMisc + 4);
   const uint32_t sbase = ptx::smem_addr(smem);
@@ -433,6 +495,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     for (int s = 0; s < kTcStages; ++s) ptx::mbar_init(&empty[s], 1);
     ptx::mbar_init(accfull, 1);
     ptx::mbar_init(done, 1);
+    ptx::mbar_init(rawfull, 1);
     *abort_flag = 0;
     ptx::fence_mbar_init();
   }
@@ -457,7 +520,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   const bool issuer = tid == 7 * 32;
   // phase-table thread: q = (tid - 256) / 8 (+ 32), nodes 2 ((tid - 256) % 8) + {0, 1}
   const int tq = (tid - 256) >> 3, tn = ((tid - 256) & 7) * 2;
-  uint32_t gst = 0;
+  uint32_t gst = 0, raw_seq = 0;
   int gbase = 0;
   TcRaw raw;
   for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
@@ -564,15 +627,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       for (uint32_t st = 0; st < nst; ++st) {
         const uint32_t g = g0 + st, s = g & (kTcStages - 1);
         const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
-        if (loader && blk + 1 < n_blocks && (j == 4 || j == 6)) {
-          const int64_t n1 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes + tid;
-          if (j == 4) {
-            if (n1 < U.n_end) tc_load_raw(p, n1, raw);
-          } else {
-            tc_derive(p, U, n1, raw, wrun, pos_all + (buf ^ 1) * 3 * kTcBlockNodes,
-                      w_all + (buf ^ 1) * WR * kWStride, tid);
-          }
-        }
+        if (loader && blk + 1 < n_blocks && (j == 4 || j == 6))
+          tc_stage_block(p, U, tid, blk, j, raw, raw_seq, smem + L.raw, rawfull, wrun,
+                         pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag);
         tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
         ptx::named_barrier(1, kTcProducers);
         if (issuer && st > 0)
@@ -617,18 +674,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       for (uint32_t st = 0; st < nst; ++st) {
         const uint32_t g = g0 + st, s = g & (kTcStages - 1);
         const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
-        if (loader && blk + 1 < n_blocks && (j == 4 || j == 6)) {
-          // block blk + 1 (block blk is then complete): raw loads issued at
-          // j == 4, derived into the other buffer at j == 6.  That buffer's
-          // readers (stages of block blk - 1) passed this block's first barrier.
-          const int64_t n1 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes + tid;
-          if (j == 4) {
-            if (n1 < U.n_end) tc_load_raw(p, n1, raw);
-          } else {
-            tc_derive(p, U, n1, raw, wrun, pos_all + (buf ^ 1) * 3 * kTcBlockNodes,
-                      w_all + (buf ^ 1) * WR * kWStride, tid);
-          }
-        }
+        // block blk + 1 (block blk is then complete): requested at j == 4,
+        // derived into the other buffer at j == 6.  That buffer's readers
+        // (stages of block blk - 1) passed this block's first barrier.
+        if (loader && blk + 1 < n_blocks && (j == 4 || j == 6))
+          tc_stage_block(p, U, tid, blk, j, raw, raw_seq, smem + L.raw, rawfull, wrun,
+                         pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag);
         // wait until the MMAs that last read stage s are done
         tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
         // every writer of the previous stage is done (its MMAs go out now); the
@@ -966,6 +1017,20 @@ __global__ void tc_write_entries_kernel(const __grid_constant__ TcEntryChunk c, 
   for (int i = threadIdx.x; i < words; i += blockDim.x) d[i] = src[i];
 }
 
+// M Mxy regrouped per column group: group g holds (N, mm_ld_g) rows with
+// mm_ld_g = its column count rounded up to even (16-byte rows for the bulk
+// copies); groups of 8 columns are consecutive.
+__global__ void tc_group_mm_kernel(const float2 *__restrict__ MM, int64_t N, int V, float2 *__restrict__ MMg) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= N * V) return;
+  const int64_t n = e / V;
+  const int v = (int)(e % V);
+  const int g = v / kTcVGroup, vi = v % kTcVGroup;
+  const int vg = (V - g * kTcVGroup) < kTcVGroup ? (V - g * kTcVGroup) : kTcVGroup;
+  const int ld = (vg + 1) & ~1;
+  MMg[(int64_t)g * N * kTcVGroup + n * ld + vi] = MM[e];
+}
+
 __global__ void tc_reduce_kernel(const float2 *__restrict__ part, const int *__restrict__ plan, int64_t count,
                                  float2 *__restrict__ out) {
   const int splits = plan[4];
@@ -984,6 +1049,7 @@ __global__ void tc_reduce_kernel(const float2 *__restrict__ part, const int *__r
 // Workspace of one problem.
 struct TcPlan {
   float *MM;
+  float2 *MMg;    // M Mxy per column group (tc_group_mm_kernel)
   Csr csr;
   Runs runs;
   float *weights;
@@ -1010,6 +1076,7 @@ static void carve_tc(Carve &c, const fm_signal_args *a, TcPlan &pl) {
   const int64_t N = a->n_nodes, V = a->n_vencs;
   pl.n_groups = tc_groups(V);
   pl.MM = c.take<float>((size_t)N * V * 2);
+  pl.MMg = c.take<float2>((size_t)pl.n_groups * N * kTcVGroup);
   carve_csr(c, a->m_rows, a->m_nnz, pl.csr);
   carve_runs(c, S, kTcRows, pl.runs);
   pl.weights = c.take<float>((size_t)(S + 1) * motion_slots(a->motion));
@@ -1097,6 +1164,10 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
   FM_TRY(build_runs<float>(static_cast<const float *>(a->t), S, kTcRows, pl.runs, st));
   FM_TRY(sparse_times_dense<float>(a, pl.csr, static_cast<const float *>(a->Mxy), pl.MM, pl.runs.error, st));
   FM_TRY(check_table_calls(a->motion, pl.runs, st));
+  tc_group_mm_kernel<<<(unsigned)ceil_div(N * V, 256), 256, 0, st>>>(reinterpret_cast<const float2 *>(pl.MM), N,
+                                                                     (int)V, pl.MMg);
+  count_launch();
+  FM_TRY(check_launch("tc_group_mm_kernel"));
   const MotionDev md = make_motion_dev(a->motion);
   FM_TRY(launch_run_weights(md, pl.runs.run_t, pl.runs.counts, S, pl.weights, st));
   const int64_t cls_blocks = S < 8 * kSmCount ? S : 8 * kSmCount;
@@ -1151,7 +1222,8 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
       p.r0 = static_cast<const float *>(a->r0);
       p.phi = static_cast<const float *>(a->phi);
       p.T2 = static_cast<const float *>(a->T2);
-      p.MM = reinterpret_cast<const float2 *>(pl.MM);
+      p.MM = pl.MMg + (size_t)g * N * kTcVGroup;
+      p.mm_ld = (VG + 1) & ~1;
       p.md = md;
       p.weights = (md.kind == FM_MOTION_TERMS) ? pl.weights : nullptr;
       p.table = (a->motion && a->motion->kind == FM_MOTION_TABLE) ? static_cast<const float *>(a->motion->table)
@@ -1170,6 +1242,11 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
       p.wrows = Rk * VG;
       int acc_cols;
       tc_shape(p.Qt, Rk * VG, p.NT, acc_cols);
+      // node blocks by bulk copies when the inputs are 16-byte aligned and the
+      // staging area fits next to the tiles
+      const bool aligned = ((uintptr_t)p.r0 % 16 == 0) && ((uintptr_t)p.T2 % 16 == 0) &&
+                           ((uintptr_t)p.phi % 16 == 0) && ((uintptr_t)p.MM % 16 == 0);
+      p.tma = aligned && tc_smem_layout(p.NT, p.wrows, p.Qt).total + tc_raw_bytes(p.mm_ld) <= kTcSmemMax;
     }
   }
   tc_plan_kernel<<<1, 32, 0, st>>>(pl.plan, pl.n_groups, N, pl.max_splits, tune ? tune->split_nodes : 0);
@@ -1203,10 +1280,11 @@ static int tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc
     int NT = host[e].NT, ac = 32;
     while (ac < NT) ac <<= 1;
     if (ac > acc_cols) acc_cols = ac;
-    const size_t sm = tc_smem_layout(NT, host[e].wrows, host[e].Qt).total;
+    const size_t sm = tc_smem_layout(NT, host[e].wrows, host[e].Qt).total +
+                      (host[e].tma ? tc_raw_bytes(host[e].mm_ld) : 0);
     if (sm > smem) smem = sm;
   }
-  FM_REQUIRE(smem <= 232448, FM_ERR_UNSUPPORTED, "%s: tile needs %zu bytes of shared memory", who, smem);
+  FM_REQUIRE(smem <= kTcSmemMax, FM_ERR_UNSUPPORTED, "%s: tile needs %zu bytes of shared memory", who, smem);
   for (int e0 = 0; e0 < ne; e0 += kTcEntriesPerWrite) {
     TcEntryChunk c;
     c.n = (ne - e0) < kTcEntriesPerWrite ? (ne - e0) : kTcEntriesPerWrite;

@@ -63,6 +63,22 @@ __device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_
   }
 }
 
+// Arrives on `bar` and adds `bytes` to the transaction count its phase waits for.
+__device__ inline void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Bulk (non-tensor, no multicast) asynchronous copy of `bytes` from global to
+// this CTA's shared memory; completion is counted in bytes on `bar`.  Both
+// addresses 16-byte aligned, bytes a multiple of 16.
+__device__ inline void bulk_copy_g2s(void *dst_smem, const void *src_gmem, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst_smem)),
+               "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
 // Generic-proxy writes to shared memory become visible to the async proxy
 // (the tensor core reading its operands).
 __device__ inline void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

@@ -96,3 +96,22 @@ def test_batch_with_empty_problem(cuda):
                             ops.Tuning(split_nodes=2048))
     assert torch.count_nonzero(outs[-1]).item() == 0
     assert all(torch.isfinite(torch.view_as_real(o)).all().item() for o in outs)
+
+
+def test_node_staging_paths_agree(cuda):
+    # node blocks are staged by bulk copies when the inputs are 16-byte
+    # aligned and by register loads otherwise; both give the same bits
+    inp, mo, _ = _batch(cuda)[1]
+    N = inp.r0.shape[0]
+    def shifted(t):
+        flat = t.reshape(-1)
+        buf = torch.empty(flat.numel() + 1, dtype=t.dtype, device=cuda)
+        buf[1:].copy_(flat)
+        return buf[1:].view(t.shape)  # 4 bytes past an aligned address
+    odd = ops.SignalInputs(M=inp.M, kx=inp.kx, ky=inp.ky, kz=inp.kz, t=inp.t, r0=shifted(inp.r0),
+                           phi=shifted(inp.phi), T2=shifted(inp.T2), Mxy=inp.Mxy)
+    assert odd.r0.data_ptr() % 16 != 0 and odd.r0.shape == (N, 3)
+    tune = ops.Tuning(split_nodes=2048)
+    a = ops.signal_batch([(inp, mo, None)], tune)[0]
+    b = ops.signal_batch([(odd, mo, None)], tune)[0]
+    np.testing.assert_array_equal(a.cpu().numpy(), b.cpu().numpy())
