@@ -170,6 +170,7 @@ SIGNATURES = {
     "fm_signal_batch_workspace_size": (C.c_int, [C.POINTER(SignalArgs), C.c_int, C.POINTER(C.c_size_t)]),
     "fm_signal_batch_enqueue": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, C.POINTER(TcTuning), _p, C.c_size_t]),
     "fm_signal_batch_status": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, _p, C.c_size_t]),
+    "fm_selftest_wait": (C.c_int, [_p, C.c_uint64]),
     "fm_mass_assemble": (C.c_int, [_p, C.POINTER(MassArgs), C.c_int, C.POINTER(_i64), _p, _p, _p, _i64, _p,
                                    C.c_size_t]),
     "fm_mass_lumped": (C.c_int, [_p, C.POINTER(MassArgs), C.c_int, _p, _p, C.c_size_t]),

@@ -1,5 +1,6 @@
 // fm_signal entry point: argument validation and dispatch over the forms.
 #include "signal_common.cuh"
+#include "tc_ptx.cuh"
 
 namespace fm {
 
@@ -101,6 +102,17 @@ int fm_signal(fm_ctx *ctx, const fm_signal_args *a, int precision, void *ws, siz
   return fm_signal_status(ctx, a, precision, ws, ws_bytes);
 }
 
+// One thread waits on an mbarrier that nothing arrives on; the bounded wait
+// runs out and the kernel records where it gave up.
+__global__ void selftest_wait_kernel(uint64_t limit_ns, int *status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  ptx::mbar_init(&bar, 1);
+  ptx::fence_mbar_init();
+  const bool done = ptx::mbar_wait(&bar, 0, limit_ns);
+  *status = done ? 0 : 1;
+}
+
 static int validate_batch(const fm_signal_args *probs, int n, const char *who) {
   FM_REQUIRE(n >= 0, FM_ERR_SHAPE, "%s: negative problem count", who);
   FM_REQUIRE(n == 0 || probs != nullptr, FM_ERR_ARG, "%s: null problem array", who);
@@ -133,6 +145,29 @@ int fm_signal_batch_status(fm_ctx *ctx, const fm_signal_args *probs, int n, void
   FM_TRY(validate_batch(probs, n, "fm_signal_batch_status"));
   DeviceGuard g(ctx->device);
   return signal_tc_batch_errors(ctx, probs, n, ws, ws_bytes);
+}
+
+int fm_selftest_wait(fm_ctx *ctx, uint64_t limit_ns) {
+  FM_TRY(ctx_ok(ctx));
+  FM_REQUIRE(limit_ns > 0 && limit_ns <= 2000000000ull, FM_ERR_ARG, "fm_selftest_wait: limit must be in (0, 2 s]");
+  DeviceGuard g(ctx->device);
+  FM_REQUIRE(g.ok, FM_ERR_CUDA, "fm_selftest_wait: cannot select device %d", ctx->device);
+  int *d = nullptr;
+  FM_CUDA(cudaMallocAsync(&d, sizeof(int), ctx->stream));
+  FM_CUDA(cudaMemsetAsync(d, 0, sizeof(int), ctx->stream));
+  selftest_wait_kernel<<<1, 32, 0, ctx->stream>>>(limit_ns, d);
+  count_launch();
+  int h = 0;
+  FM_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  FM_CUDA(cudaFreeAsync(d, ctx->stream));
+  FM_CUDA(cudaStreamSynchronize(ctx->stream));
+  FM_TRY(check_launch("selftest_wait_kernel"));
+  if (h != 0) {
+    set_error(FM_ERR_TIMEOUT, "fm_selftest_wait: the device wait ran out after %llu ns (expected)",
+              (unsigned long long)limit_ns);
+    return FM_ERR_TIMEOUT;
+  }
+  return FM_OK;
 }
 
 int64_t fm_signal_count_time_runs(const void *t_host, int64_t n_samples, int is_double) {

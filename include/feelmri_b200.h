@@ -258,6 +258,15 @@ FM_API int fm_signal_status(fm_ctx *ctx, const fm_signal_args *args, int precisi
                             void *workspace, size_t workspace_bytes);
 FM_API int fm_signal_workspace_size(const fm_signal_args *args, int precision,
                              size_t *bytes);
+/* Self-test of the bounded device waits the tensor-core kernels use (no
+ * counterpart in the reference): one thread waits on an mbarrier that
+ * nothing arrives on, gives up after `limit_ns` of device wall time and
+ * records the timeout; the call returns FM_ERR_TIMEOUT (the expected
+ * outcome) after synchronising the context's stream.  The context and the
+ * device stay usable.  Lets a host check its failure handling without a
+ * GPU fault. */
+FM_API int fm_selftest_wait(fm_ctx *ctx, uint64_t limit_ns);
+
 /* Batched split-BF16 Signal (no counterpart in the reference, which calls
  * Signal once per phantom, e.g. examples/phase_contrast.py:207): n problems,
  * each an fm_signal_args with its own mesh, trajectory, columns, motion and

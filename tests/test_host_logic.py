@@ -1,0 +1,90 @@
+"""Host-side logic that needs no GPU: the autotuner's shape classes and cache
+file, the serving loop's footprint and latency statistics, the SPAMM block's
+physics (through the FP64 oracle) and the batching workload generator."""
+import json
+
+import numpy as np
+import torch
+
+from oracle import fp64
+from feelmri_b200 import autotune, ops, workloads as W
+from feelmri_b200.serving import Request, footprint_bytes, latency_stats
+
+
+def _fake_problem(N, grid, V):
+    z = lambda *s: torch.zeros(*s)  # noqa: E731
+    inp = ops.SignalInputs(M=None, kx=z(grid), ky=z(grid), kz=z(grid), t=z(grid), r0=z(N, 3), phi=z(N), T2=z(N),
+                           Mxy=torch.zeros(N, V, dtype=torch.complex64))
+    return (inp, None, None)
+
+
+def test_shape_class_buckets():
+    a = [_fake_problem(10_000, (8, 16, 8), 2), _fake_problem(20_000, (8, 16, 8), 1)]
+    b = [_fake_problem(10_500, (8, 16, 8), 2), _fake_problem(19_000, (8, 16, 8), 1)]
+    c = [_fake_problem(10_000, (8, 16, 8), 4), _fake_problem(20_000, (8, 16, 8), 1)]
+    assert autotune.shape_class(a) == autotune.shape_class(b)  # same log2 buckets
+    assert autotune.shape_class(a) != autotune.shape_class(c)  # wider columns
+    assert autotune.shape_class(a) != autotune.shape_class(a[:1])
+
+
+def test_tuning_cache_file_round_trip(tmp_path, monkeypatch):
+    path = tmp_path / "tuning.json"
+    monkeypatch.setenv("FEELMRI_B200_TUNING", str(path))
+    monkeypatch.setattr(autotune, "_cache", {})
+    probs = [_fake_problem(50_000, (32, 32, 16), 2)]
+    key = autotune.shape_class(probs)
+    autotune._cache[key] = ops.Tuning(split_nodes=8192, kz_cap=16)
+    autotune._store()
+    assert json.loads(path.read_text())[key] == {"split_nodes": 8192, "kz_cap": 16}
+    monkeypatch.setattr(autotune, "_cache", {})
+    assert autotune.cached(probs) == ops.Tuning(split_nodes=8192, kz_cap=16)
+    # a cached batch class is returned without timing anything
+    tuning, tried = autotune.tune(probs)
+    assert tuning == ops.Tuning(split_nodes=8192, kz_cap=16) and tried == {}
+
+
+def test_candidates_are_valid_tunings():
+    assert len(set(autotune.CANDIDATES)) == len(autotune.CANDIDATES)
+    for t in autotune.CANDIDATES:
+        s = t.struct()
+        assert s.split_nodes == t.split_nodes >= 0 and s.kz_cap == t.kz_cap >= 0
+
+
+def test_latency_stats_and_footprint():
+    st = latency_stats([0.1, 0.2, 0.3, 0.4])
+    assert st["n"] == 4 and abs(st["p50_s"] - 0.25) < 1e-12 and st["p99_s"] <= 0.4 + 1e-12
+    assert latency_stats([])["n"] == 0
+    mesh = W.cylinder(2000)
+    N = mesh.n_nodes
+    T1, T2 = W.tissue(N, 0)
+
+    def req(traj, coils):
+        return Request(rid=0, mesh=mesh, T1=T1, T2=T2, phi=np.zeros(N, np.float32), blocks=[], traj=traj,
+                       coils=np.ones((N, coils), np.complex64))
+    small = footprint_bytes(req(W.cartesian(res=(8, 8, 8)), 1))
+    big = footprint_bytes(req(W.cartesian(res=(32, 32, 8)), 4))
+    assert 0 < small < big
+
+
+def test_spamm_block_tags_mz():
+    b = W.spamm_block(0.0, tag_spacing=0.008, tail=0.1)
+    x = np.linspace(-0.02, 0.02, 81)
+    r0 = np.stack([x, np.zeros_like(x), np.zeros_like(x)], 1).astype(np.float32)
+    N = x.size
+    slow = np.full(N, 1e9, np.float32)  # no relaxation
+    res = fp64.bloch(r0, slow, slow, np.zeros(N, np.float32), 1.0, W.GAMMA, b.rf, b.G, b.dt.astype(np.float32),
+                     np.zeros(N, np.complex64), np.ones(N, np.float32))
+    Mz = np.asarray(res[1] if isinstance(res, tuple) else res).reshape(N, -1)[:, -1]
+    ke = 2 * np.pi / 0.008
+    np.testing.assert_allclose(Mz, -np.cos(ke * x), atol=1e-5)
+
+
+def test_batching_workload_is_seeded_and_in_range():
+    import bench
+    a = bench.build_batch_case(n_phantoms=6)
+    b = bench.build_batch_case(n_phantoms=6)
+    assert [c["N"] for c in a] == [c["N"] for c in b]
+    for c in a:
+        assert 4_000 <= c["N"] <= 320_000
+        assert 1 <= c["coils"].shape[1] <= 2
+        assert c["traj"].shape[2] >= 8  # every trajectory is a kz stack (factorable slabs)
