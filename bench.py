@@ -227,6 +227,32 @@ def run_gpu(args) -> dict | None:
     got = out.cpu().numpy().reshape(S, V)[idx]
     rel = fp64.rel_l2(got, ref)
 
+    # Bloch sweep in its API-exact history form (HBM-bound: every node-step
+    # writes c64 Mxy + f32 Mz): one encoding block, timed alone, untimed by
+    # the step.  Algorithmic bytes = N n_t 12 written + N 36 read (position,
+    # T1, T2, dB, initial state) + n_t 24 (rf, G, dt) + the rank-1 modes.
+    rf, G, dt, t0 = blocks[1]
+    vel.update_timeshift(frame_ms * rank + t0)
+    hist_motion = lower(vel, N, dev)
+    hinp = ops.BlochInputs(r0=r0, T1=T1, T2=T2, delta_B=dB, M0=1.0, gamma=W.GAMMA, rf=rf, G=G, dt=dt,
+                           Mxy0=zero_m, Mz0=one_z)
+    ops.bloch_solve(hinp, hist_motion, history=True)
+    torch.cuda.synchronize(dev)
+    h_ms = []
+    for _ in range(5):
+        flush.zero_()
+        a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a_ev.record(stream)
+        ops.bloch_solve(hinp, hist_motion, history=True)
+        b_ev.record(stream)
+        b_ev.synchronize()
+        h_ms.append(a_ev.elapsed_time(b_ev))
+    n_t = int(rf.shape[0])
+    h_bytes = float(N) * n_t * 12 + float(N) * (12 + 12 + 12 + 12) + n_t * 24
+    bloch_hist = {"bound": "hbm", "ms": statistics.median(h_ms), "bytes": h_bytes,
+                  "achieved": h_bytes / (statistics.median(h_ms) / 1e3) / 1e9, "unit": "GB/s",
+                  "node_steps_per_s": float(N) * n_t / (statistics.median(h_ms) / 1e3), "n_t": n_t}
+
     result = None
     if rank == 0:
         units = float(N) * S * world
@@ -266,6 +292,8 @@ def run_gpu(args) -> dict | None:
             "rel_l2_vs_fp64": rel,
             "roofline": roof,
             "bloch_ms_per_step": b_ms / args.steps,
+            "bloch_history_roofline": dict(bloch_hist, peak=peaks["hbm_gbs"],
+                                           frac=bloch_hist["achieved"] / peaks["hbm_gbs"]),
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
         }
