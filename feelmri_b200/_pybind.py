@@ -110,8 +110,20 @@ def sequence_of(obj, fn):
 
 
 def sparse_csc(obj, dtype):
-    """Eigen SparseMatrix<T> (column-major) caster."""
+    """Eigen SparseMatrix<T> (column-major) caster.
+
+    A float lil_matrix (the lumped mass of the reference's examples) is
+    converted by the native _hostconv.lil_to_csc, which yields the arrays of
+    scipy.sparse.csc_matrix(obj); every other input, and any lil that the
+    native pass declines, goes through scipy."""
     import scipy.sparse as sp
+    if isinstance(obj, sp.lil_matrix) and obj.dtype in (np.float64, np.float32):
+        fast = _lil_to_csc(obj)
+        if fast is not None:
+            indptr, indices, data = fast
+            if data.dtype != np.dtype(dtype):
+                data = _force_cast(data.astype(obj.dtype, copy=False), np.dtype(dtype))
+            return obj.shape, indptr, indices, data
     try:
         if type(obj) is not sp.csc_matrix:
             obj = sp.csc_matrix(obj)
@@ -123,6 +135,15 @@ def sparse_csc(obj, dtype):
     indices = np.asarray(obj.indices).astype(np.int32, copy=False)
     indptr = np.asarray(obj.indptr).astype(np.int32, copy=False)
     return obj.shape, indptr, indices, data
+
+
+def _lil_to_csc(m):
+    try:
+        from . import _hostconv
+    except ImportError as exc:
+        raise ImportError("feelmri_b200._hostconv is not built; run `python -m feelmri_b200.build`") from exc
+    n_rows, n_cols = m.shape
+    return _hostconv.lil_to_csc(m.rows, m.data, n_rows, n_cols)
 
 
 def py_float(obj, convert: bool) -> float:

@@ -72,6 +72,25 @@ def build(verbose: bool = False, extra_flags=None, jobs: int = 8) -> Path:
     return LIB
 
 
+def build_host(verbose: bool = False) -> Path:
+    """Compiles the CPython extension _hostconv (host-side argument
+    conversion, csrc/hostconv.cpp) with g++ next to the package."""
+    import sysconfig
+    import numpy as np
+    src = CSRC / "hostconv.cpp"
+    out = PKG / ("_hostconv" + sysconfig.get_config_var("EXT_SUFFIX"))
+    if out.exists() and out.stat().st_mtime > max(src.stat().st_mtime, Path(__file__).stat().st_mtime):
+        return out
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden", "-pthread",
+           "-I", sysconfig.get_paths()["include"], "-I", np.get_include(), str(src), "-o", str(out)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("g++ failed on hostconv.cpp:\n" + res.stdout)
+    return out
+
+
 def _drain(procs):
     failed = []
     for name, p in procs:
@@ -87,3 +106,4 @@ def _drain(procs):
 
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))
+    print(build_host(verbose="-v" in sys.argv))

@@ -88,3 +88,66 @@ def test_batching_workload_is_seeded_and_in_range():
         assert 4_000 <= c["N"] <= 320_000
         assert 1 <= c["coils"].shape[1] <= 2
         assert c["traj"].shape[2] >= 8  # every trajectory is a kz stack (factorable slabs)
+
+
+def _csc_arrays(m, dtype):
+    import scipy.sparse as sp
+    c = sp.csc_matrix(m)
+    return c.shape, c.indptr.astype(np.int32), c.indices.astype(np.int32), c.data.astype(dtype)
+
+
+def test_lil_conversion_matches_scipy():
+    # the Signal caster converts a float lil_matrix natively; the arrays must be
+    # exactly those of scipy.sparse.csc_matrix(lil) with the data force-cast
+    import scipy.sparse as sp
+    from feelmri_b200 import _hostconv, _pybind as pb
+    rng = np.random.default_rng(7)
+    cases = []
+    N = 5000
+    D = sp.lil_matrix((N, N), dtype=np.float64)
+    D.setdiag(rng.uniform(1e-7, 3e-7, N))
+    cases.append(D)                                               # the lumped mass: a diagonal
+    for seed, dt in ((1, np.float64), (2, np.float32)):
+        R = sp.random(700, 400, density=0.02, random_state=seed, format="lil", dtype=dt)
+        R[3, :] = 0                                               # an empty row
+        cases.append(R)                                           # general pattern: the scatter path
+    P = sp.lil_matrix((6, 4), dtype=np.float64)
+    P[0, 2], P[1, 0], P[5, 3] = 1.0, -2.0, 3.0                    # not monotone in row order
+    cases.append(P)
+    cases.append(sp.lil_matrix((0, 0)))
+    cases.append(sp.lil_matrix((5, 3)))
+    for m in cases:
+        for T in (np.float32, np.float64):
+            got = pb.sparse_csc(m, T)
+            want = _csc_arrays(m, T)
+            assert got[0] == want[0]
+            for g, w in zip(got[1:], want[1:]):
+                assert g.dtype == w.dtype
+                np.testing.assert_array_equal(g, w)
+        for threads in (1, 3):
+            r = _hostconv.lil_to_csc(m.rows, m.data, m.shape[0], m.shape[1], threads)
+            c = sp.csc_matrix(m)
+            np.testing.assert_array_equal(r[0], c.indptr)
+            np.testing.assert_array_equal(r[1], c.indices)
+            np.testing.assert_array_equal(r[2], c.data.astype(np.float64))
+
+
+def test_lil_conversion_declines_what_scipy_must_handle():
+    import scipy.sparse as sp
+    from feelmri_b200 import _hostconv, _pybind as pb
+    m = sp.lil_matrix((4, 4), dtype=np.float64)
+    m[1, 2] = 5.0
+    rows = m.rows.copy()
+    rows[0] = [3]                                                 # lists of unequal length
+    assert _hostconv.lil_to_csc(rows, m.data, 4, 4) is None
+    rows = m.rows.copy()
+    rows[1] = [9]
+    assert _hostconv.lil_to_csc(rows, m.data, 4, 4) is None       # column index >= n_cols
+    data = m.data.copy()
+    data[1] = ["x"]
+    assert _hostconv.lil_to_csc(m.rows, data, 4, 4) is None       # a value that is not a number
+    # complex lil goes through scipy and the caster's real-part cast
+    z = sp.lil_matrix((3, 3), dtype=np.complex128)
+    z[0, 0] = 1 + 2j
+    got = pb.sparse_csc(z, np.float32)
+    np.testing.assert_array_equal(got[3], np.array([1.0], np.float32))
