@@ -343,10 +343,16 @@ def run_e2e(args, case, w, precision) -> dict:
         K = step()
     torch.cuda.synchronize()
     dt = (time.perf_counter() - t0) / n
-    h2d = (nodes32.nbytes * 2 + case["T1"].nbytes + case["T2"].nbytes * 2 + case["dB"].nbytes + case["phi"].nbytes
+    V = K.shape[-1]
+    n_blocks = len(case["blocks"])
+    # per solver: nodes, T1, T2, delta_B (initial state is filled on the device);
+    # per block: rf, G, dt.  Signal: M (indptr, indices, data), k-space and
+    # times, nodes, phi, T2 and the Mxy columns.
+    h2d = (n_blocks * (nodes32.nbytes + 3 * N * 4)
            + sum(b.rf.nbytes + b.G.nbytes + b.dt.astype(np.float32).nbytes for b in case["blocks"])
-           + sum(p.nbytes for p in traj.points) + traj.t.nbytes + N * 4 * 8 + N * 8 + (N + 1) * 4 + N * 4)
-    d2h = K.nbytes + 4 * N * (8 + 4)
+           + (N + 1) * 4 + N * 4 + N * 4 + sum(p.nbytes for p in traj.points) + traj.t.nbytes
+           + nodes32.nbytes + 2 * N * 4 + N * V * 8)
+    d2h = K.nbytes + n_blocks * N * (8 + 4)
     return {"value": float(N) * traj.n_samples / dt, "unit": "node*k-sample/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "timer": "host wall clock around the public calls, device synchronised"}
 

@@ -47,39 +47,102 @@ def discretise(block):
     return times, rf, Gm, t0
 
 
+_STATE = {"initial_Mxy": (np.complex64, torch.complex64), "initial_Mz": (np.float32, torch.float32)}
+_PARAMS = ("T1", "T2", "delta_B")
+
+
 class BlochSolver:
+    """Per-node parameters and the carried state live on the device.
+
+    T1, T2, delta_B, initial_Mxy and initial_Mz read as the reference's (N, 1)
+    host arrays (Bloch.py:285-293), built on first access.  Values are taken
+    at construction: scalars are filled on the device, arrays uploaded once.
+    The carried state stays on the GPU between solves.  Once a host array has
+    been read it is the one the next solve starts from, so in-place edits take
+    effect, and each solve writes the carried state back into initial_Mxy /
+    initial_Mz in place, as the reference does (Bloch.py:363-368).  Arrays
+    that were never read are never copied to the host."""
+
     def __init__(self, blocks, nodes, M0=1.0, T1=1000.0, T2=100.0, delta_B=0.0, gamma=267.522, pod_trajectory=None,
                  initial_Mxy=0.0, initial_Mz=None, device=None):
         self.blocks = list(blocks)
-        nodes = np.asarray(nodes)
-        N = nodes.shape[0]
-        ones = np.ones((N, 1), np.float32)
-        self.nodes = nodes
+        self.nodes = np.asarray(nodes)
         self.M0 = M0
         self.gamma = gamma
-        self.T1 = np.asarray(T1, np.float32).reshape(-1, 1) * ones if np.ndim(T1) else T1 * ones
-        self.T2 = np.asarray(T2, np.float32).reshape(-1, 1) * ones if np.ndim(T2) else T2 * ones
-        self.delta_B = np.asarray(delta_B, np.float32).reshape(-1, 1) * ones if np.ndim(delta_B) else delta_B * ones
-        self.initial_Mxy = (np.asarray(initial_Mxy).reshape(-1, 1) * ones).astype(np.complex64)
-        self.initial_Mz = (np.asarray(initial_Mz if initial_Mz is not None else M0).reshape(-1, 1) * ones).astype(
-            np.float32)
         self.pod_trajectory = pod_trajectory
         self.device = device or ops.require_cuda()
-        self._dev_static = None
+        self._given = {"T1": T1, "T2": T2, "delta_B": delta_B, "initial_Mxy": initial_Mxy,
+                       "initial_Mz": initial_Mz if initial_Mz is not None else M0}
+        self._host: dict[str, np.ndarray] = {}
+        self._dev: dict[str, torch.Tensor] = {}
+        self._dev_nodes = torch.from_numpy(np.ascontiguousarray(self.nodes, dtype=np.float32)).to(self.device)
+        for name in (*_PARAMS, *_STATE):
+            self._dev[name] = self._snapshot(name)
 
     @property
     def n_nodes(self) -> int:
         return self.nodes.shape[0]
 
-    def _static(self):
-        if self._dev_static is None:
-            dev = self.device
+    def _construct(self, name: str) -> np.ndarray:
+        """The (N, 1) host array the reference builds (Bloch.py:285-293)."""
+        ones = np.ones((self.n_nodes, 1), np.float32)
+        v = self._given[name]
+        if name in _STATE:
+            return (np.asarray(v).reshape(-1, 1) * ones).astype(_STATE[name][0])
+        return np.asarray(v, np.float32).reshape(-1, 1) * ones if np.ndim(v) else v * ones
 
-            def up(a, dt=torch.float32):
-                return torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dt)
-            self._dev_static = dict(r0=up(self.nodes.astype(np.float32)), T1=up(self.T1.reshape(-1)),
-                                    T2=up(self.T2.reshape(-1)), dB=up(self.delta_B.reshape(-1)))
-        return self._dev_static
+    def _snapshot(self, name: str) -> torch.Tensor:
+        """(N,) device copy of the constructed value: a fill for one value, an
+        upload otherwise (an array of N parameter values is uploaded as given:
+        multiplying it by ones leaves it unchanged)."""
+        N = self.n_nodes
+        np_t, torch_t = _STATE.get(name, (np.float32, torch.float32))
+        v = self._given[name]
+        if np.size(v) == 1:
+            if name in _STATE:
+                one = (np.asarray(v).reshape(-1, 1) * np.ones((1, 1), np.float32)).astype(np_t)
+            elif np.ndim(v):
+                one = np.asarray(v, np.float32)
+            else:
+                one = np.asarray(v * np.ones((1, 1), np.float32))
+            return torch.full((N,), one.reshape(-1)[0].item(), dtype=torch_t, device=self.device)
+        if name not in _STATE and np.size(v) == N:
+            flat = np.asarray(v, np.float32).reshape(-1)
+        else:
+            flat = self._construct(name).reshape(-1)
+        return self._upload(flat, np_t)
+
+    def _upload(self, flat: np.ndarray, np_t) -> torch.Tensor:
+        if flat.size != self.n_nodes:
+            raise ValueError(f"BlochSolver: {flat.size} values for {self.n_nodes} nodes")
+        return torch.from_numpy(np.ascontiguousarray(flat.astype(np_t, copy=False))).to(self.device)
+
+    def _host_array(self, name: str) -> np.ndarray:
+        if name not in self._host:
+            if name in _STATE:
+                self._host[name] = self._dev[name].cpu().numpy().reshape(self.n_nodes, 1)
+            else:
+                self._host[name] = self._construct(name)
+        return self._host[name]
+
+    def _set_host(self, name: str, value) -> None:
+        self._host[name] = np.asarray(value)
+
+    T1 = property(lambda self: self._host_array("T1"), lambda self, v: self._set_host("T1", v))
+    T2 = property(lambda self: self._host_array("T2"), lambda self, v: self._set_host("T2", v))
+    delta_B = property(lambda self: self._host_array("delta_B"), lambda self, v: self._set_host("delta_B", v))
+    initial_Mxy = property(lambda self: self._host_array("initial_Mxy"),
+                           lambda self, v: self._set_host("initial_Mxy", v))
+    initial_Mz = property(lambda self: self._host_array("initial_Mz"),
+                          lambda self, v: self._set_host("initial_Mz", v))
+
+    def _device_array(self, name: str) -> torch.Tensor:
+        """The value a solve starts from: the host array when one has been
+        handed out (it may have been edited), else the device copy."""
+        if name in self._host:
+            self._dev[name] = self._upload(np.asarray(self._host[name]).reshape(-1),
+                                           _STATE.get(name, (np.float32,))[0])
+        return self._dev[name]
 
     def solve(self, start: int = 0, end: int | None = None):
         if start < 0:
@@ -89,18 +152,19 @@ class BlochSolver:
         blocks = self.blocks[start:end]
         N = self.n_nodes
         dev = self.device
-        st = self._static()
+        r0 = self._dev_nodes
+        T1, T2, dB = (self._device_array(n) for n in _PARAMS)
         store = [i for i, b in enumerate(blocks) if b.store_magnetization]
         out_m = torch.zeros((max(len(store), 1), N), dtype=torch.complex64, device=dev)
         out_z = torch.zeros((max(len(store), 1), N), dtype=torch.float32, device=dev)
-        m = torch.from_numpy(self.initial_Mxy.reshape(-1).copy()).to(dev)
-        z = torch.from_numpy(self.initial_Mz.reshape(-1).copy()).to(dev)
+        m = self._device_array("initial_Mxy")
+        z = self._device_array("initial_Mz")
         for i, block in enumerate(blocks):
             times, rf, G, t0 = discretise(block)
             if self.pod_trajectory is not None:
                 self.pod_trajectory.update_timeshift(t0)
             dt = np.diff(times, prepend=0).astype(np.float32)
-            inp = ops.BlochInputs(r0=st["r0"], T1=st["T1"], T2=st["T2"], delta_B=st["dB"], M0=self.M0,
+            inp = ops.BlochInputs(r0=r0, T1=T1, T2=T2, delta_B=dB, M0=self.M0,
                                   gamma=self.gamma, rf=torch.from_numpy(rf).to(dev),
                                   G=torch.from_numpy(np.ascontiguousarray(G)).to(dev),
                                   dt=torch.from_numpy(dt).to(dev), Mxy0=m, Mz0=z)
@@ -119,8 +183,14 @@ class BlochSolver:
                 z.copy_(fin_z)
                 if empty:
                     m.copy_(fin_m)
-        self.initial_Mxy[:, 0] = m.cpu().numpy()
-        self.initial_Mz[:, 0] = z.cpu().numpy()
+        for name, t in (("initial_Mxy", m), ("initial_Mz", z)):
+            if name in self._host:  # handed out: updated in place, as the reference does
+                host = self._host[name]
+                if host.ndim == 2:
+                    host[:, 0] = t.cpu().numpy()
+                else:
+                    host[...] = t.cpu().numpy().reshape(host.shape)
         if not store:
             return np.zeros((N, 0), np.complex64), np.zeros((N, 0), np.float32)
-        return out_m.cpu().numpy().T, out_z.cpu().numpy().T
+        host_m, host_z = ops.to_host(out_m, out_z)
+        return host_m.T, host_z.T

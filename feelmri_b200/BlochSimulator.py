@@ -95,4 +95,5 @@ def _run(r0, T1, T2, delta_B, M0, gamma, rf, G, dt, regime, Mxy0, Mz0, pod):
         motion = table_motion(table)
     Mxy_h, Mz_h = ops.bloch_solve(inp, motion, history=True)
     # (n_t, N) row-major on the device == (N, n_t) column-major
-    return Mxy_h.cpu().numpy().T, Mz_h.cpu().numpy().T
+    m, z = ops.to_host(Mxy_h, Mz_h)
+    return m.T, z.T

@@ -106,4 +106,4 @@ def _run(rank, M, kloc, t, r0, phi, T2, Mxy, pod, T, precision):
         table = sample_table(pod, calls, N, T, dev)
         motion = table_motion(table[1:].contiguous())  # the first call's result is unused
     out = ops.signal(inp, motion, prec)
-    return out.cpu().numpy()
+    return ops.to_host(out)

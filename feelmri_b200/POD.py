@@ -35,4 +35,4 @@ def tensordot_modes_weights(modes, weights):
     dev = ops.require_cuda()
     m = torch.from_numpy(modes).to(dev)
     w = torch.from_numpy(weights).to(dev)
-    return ops.tensordot_modes_weights(m, w).cpu().numpy()
+    return ops.to_host(ops.tensordot_modes_weights(m, w))

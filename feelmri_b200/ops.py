@@ -53,6 +53,27 @@ def release_workspaces() -> None:
     _ws_cache.clear()
 
 
+PINNED_RESULT_MAX = 256 << 20
+
+
+def to_host(*tensors: torch.Tensor):
+    """Device results as numpy arrays through pinned staging: the copies are
+    queued on the current stream and waited for once.  The arrays keep their
+    pinned buffers (torch's caching host allocator takes them back when the
+    arrays die); results above PINNED_RESULT_MAX bytes in total are copied to
+    pageable memory instead, so that held results do not pin large amounts of
+    host memory."""
+    if sum(t.numel() * t.element_size() for t in tensors) > PINNED_RESULT_MAX:
+        out = [t.cpu().numpy() for t in tensors]
+    else:
+        staged = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in tensors]
+        for h, t in zip(staged, tensors):
+            h.copy_(t, non_blocking=True)
+        torch.cuda.current_stream(tensors[0].device).synchronize()
+        out = [h.numpy() for h in staged]
+    return out[0] if len(out) == 1 else tuple(out)
+
+
 def _ptr(t: torch.Tensor | None) -> int | None:
     return None if t is None else t.data_ptr()
 

@@ -74,3 +74,45 @@ def test_solver_matches_reference_block_loop(cuda, with_motion):
     rm2, rz2, _, _ = _reference_loop(blocks[-2:], nodes, T1, T2, dB, ref_pod, gm0, gz0)
     assert fp64.rel_l2(m2, rm2) < 3e-6
     assert fp64.rel_l2(z2, rz2) < 3e-6
+
+
+def _small_case():
+    mesh = W.cylinder(2000)
+    N = mesh.n_nodes
+    T1, T2 = W.tissue(N)
+    return mesh.nodes.astype(np.float32), N, T1, T2, _blocks()[:4]
+
+
+def test_scalar_and_array_parameters_agree(cuda):
+    # scalars are filled on the device, arrays uploaded: same bits either way
+    nodes, N, _, _, blocks = _small_case()
+    a = BlochSolver(blocks, nodes, M0=1.0, T1=900.0, T2=80.0, delta_B=0.0, gamma=W.GAMMA)
+    b = BlochSolver(blocks, nodes, M0=1.0, T1=np.full(N, 900.0, np.float32), T2=np.full((N, 1), 80.0),
+                    delta_B=np.zeros(N), gamma=W.GAMMA, initial_Mxy=np.zeros(N), initial_Mz=np.ones(N))
+    ma, za = a.solve()
+    mb, zb = b.solve()
+    np.testing.assert_array_equal(ma, mb)
+    np.testing.assert_array_equal(za, zb)
+    # host views keep the reference's construction: (N, 1) arrays
+    assert a.T1.shape == (N, 1) and a.T1.dtype == np.float32 and a.initial_Mxy.dtype == np.complex64
+    np.testing.assert_array_equal(a.initial_Mxy, b.initial_Mxy)
+
+
+def test_state_arrays_follow_the_reference(cuda):
+    # a held initial_Mz is updated in place by each solve; an in-place edit of
+    # initial_Mxy is what the next solve starts from (Bloch.py:363-368)
+    nodes, N, T1, T2, blocks = _small_case()
+    s = BlochSolver(blocks, nodes, M0=1.0, T1=T1, T2=T2, gamma=W.GAMMA)
+    held = s.initial_Mz
+    s.solve()
+    fresh = BlochSolver(blocks, nodes, M0=1.0, T1=T1, T2=T2, gamma=W.GAMMA)
+    fresh.solve()
+    np.testing.assert_array_equal(held, fresh.initial_Mz)   # written back in place
+    edit = (np.random.default_rng(3).normal(size=N) * 0.1).astype(np.complex64)
+    s.initial_Mxy[:, 0] = edit
+    m1, z1 = s.solve(start=-1)
+    t = BlochSolver(blocks, nodes, M0=1.0, T1=T1, T2=T2, gamma=W.GAMMA, initial_Mxy=edit,
+                    initial_Mz=fresh.initial_Mz[:, 0].copy())
+    m2, z2 = t.solve(start=-1)
+    np.testing.assert_array_equal(m1, m2)
+    np.testing.assert_array_equal(z1, z2)
