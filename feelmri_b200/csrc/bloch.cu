@@ -54,7 +54,9 @@ struct BlochDev {
 };
 
 // MODE: 0 static, 1 TERMS with the POD modes of one term in registers,
-//       2 TERMS read from global memory (several POD terms), 3 TABLE.
+//       2 TERMS read from global memory (several POD terms), 3 TABLE,
+//       4 one POD term and nothing else (modes in registers; the common
+//         pod_trajectory of the examples): no per-step term loop.
 template <int MODE, int RMAX, bool HIST>
 __global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -73,7 +75,7 @@ __global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
 
   float phx[RMAX > 0 ? RMAX : 1], phy[RMAX > 0 ? RMAX : 1], phz[RMAX > 0 ? RMAX : 1];
   int r_pod = 0;
-  if (MODE == 1) {
+  if (MODE == 1 || MODE == 4) {
     const fm_motion_term &T = p.md.terms[p.pod_term];
     r_pod = T.n_modes;
     const float *Phi = T.modes + (size_t)n * 3 * r_pod;
@@ -86,17 +88,40 @@ __global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
   }
 
   float e1 = 0.f, e2 = 0.f;
-  const int64_t steps = p.n_time - 1;
-  for (int64_t i = 0; i < steps; ++i) {
-    const float4 a = p.sa[i];
-    const float4 b = p.sb[i];
-    if (p.changed[i]) {
+  // 32-bit step counter and running pointers (n_time < 2^31 is checked on
+  // the host): the per-step addressing is a few pointer increments.
+  const int steps = (int)(p.n_time - 1);
+  const float4 *sa = p.sa, *sb = p.sb;
+  const int *chg = p.changed;
+  const float *wrow = (MODE == 4) ? p.weights + p.md.slots + p.md.slot0[p.pod_term] : nullptr;
+  float2 *hist_m = HIST ? p.Mxy_hist + n : nullptr;
+  float *hist_z = HIST ? p.Mz_hist + n : nullptr;
+  for (int i = 0; i < steps; ++i, ++sa, ++sb, ++chg) {
+    const float4 a = *sa;
+    const float4 b = *sb;
+    if (HIST) {
+      hist_m += p.n;
+      hist_z += p.n;
+    }
+    if (*chg) {
       e1 = expf(__fmul_rn(-b.w, invT1));
       e2 = expf(__fmul_rn(-b.w, invT2));
     }
     float px = x, py = y, pz = z;
-    if (MODE == 1 || MODE == 2) {
-      const float *w = p.weights + (i + 1) * p.md.slots;
+    if (MODE == 4) {
+      // the single term's sum, as the k == 0 case of the term loop below
+      float tx = 0.f, ty = 0.f, tz = 0.f;
+#pragma unroll
+      for (int m = 0; m < RMAX; ++m) {
+        const float wm = (m < r_pod) ? wrow[m] : 0.f;
+        tx = fmaf(phx[m], wm, tx);
+        ty = fmaf(phy[m], wm, ty);
+        tz = fmaf(phz[m], wm, tz);
+      }
+      wrow += p.md.slots;
+      px = __fadd_rn(x, tx); py = __fadd_rn(y, ty); pz = __fadd_rn(z, tz);
+    } else if (MODE == 1 || MODE == 2) {
+      const float *w = p.weights + (int64_t)(i + 1) * p.md.slots;
       float sx = 0.f, sy = 0.f, sz = 0.f;
       for (int k = 0; k < p.md.n_terms; ++k) {
         const fm_motion_term &T = p.md.terms[k];
@@ -132,11 +157,37 @@ __global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
       }
       px = __fadd_rn(x, sx); py = __fadd_rn(y, sy); pz = __fadd_rn(z, sz);
     } else if (MODE == 3) {
-      const float *d = p.table + ((i + 1) * p.n + n) * 3;
+      const float *d = p.table + ((int64_t)(i + 1) * p.n + n) * 3;
       px = __fadd_rn(x, d[0]); py = __fadd_rn(y, d[1]); pz = __fadd_rn(z, d[2]);
     }
     // Bz = r . G + dB  (BlochSimulator.cpp:104-107)
     const float Bz = __fadd_rn(fmaf(pz, b.z, fmaf(py, b.y, __fmul_rn(px, b.x))), db);
+    if (a.x == 0.f && a.y == 0.f) {
+      // No RF on this step (the same for every thread): beta = 0, so the
+      // update reduces to Mxy' = conj(alpha)^2 Mxy, Mz' = |alpha|^2 Mz; the
+      // dropped terms of the general form below are exact zeros.  |rf|^2 is
+      // 0, and sqrt(RN(Bz^2)) = |Bz| exactly whenever Bz^2 is a normal float
+      // (checked for every float32 mantissa), so the norm needs no sqrt.
+      const float aBz = fabsf(Bz);
+      float Bn = (aBz >= 1e-18f && aBz <= 1e18f) ? aBz : sqrtf(__fmul_rn(Bz, Bz));
+      Bn = (Bn < 1e-12f) ? 1e-12f : Bn;
+      const float nz = __fmul_rn(Bz, __frcp_rn(Bn));
+      float s, c;
+      sincosf(__fmul_rn(Bn, a.w), &s, &c);
+      const float ca_i = nz * s;  // conj(alpha) = c + i nz s
+      const float a2 = fmaf(c, c, ca_i * ca_i);
+      const float ca2r = c * c - ca_i * ca_i, ca2i = 2.f * c * ca_i;
+      const float nmr = ca2r * mxy.x - ca2i * mxy.y;
+      const float nmi = ca2r * mxy.y + ca2i * mxy.x;
+      mxy.x = nmr * e2;
+      mxy.y = nmi * e2;
+      mz = fmaf(a2 * mz, e1, (1.f - e1) * M0);
+      if (HIST) {
+        *hist_m = mxy;
+        *hist_z = mz;
+      }
+      continue;
+    }
     float Bn = sqrtf(fmaf(Bz, Bz, a.z));
     Bn = (Bn < 1e-12f) ? 1e-12f : Bn;
     const float invB = __frcp_rn(Bn);
@@ -174,8 +225,8 @@ __global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
     mxy.y = nmi * e2;
     mz = fmaf(nmz, e1, (1.f - e1) * M0);
     if (HIST) {
-      p.Mxy_hist[(i + 1) * p.n + n] = mxy;
-      p.Mz_hist[(i + 1) * p.n + n] = mz;
+      *hist_m = mxy;
+      *hist_z = mz;
     }
   }
   if (p.Mxy_final) p.Mxy_final[n * p.final_stride] = mxy;
@@ -206,6 +257,8 @@ static int validate_bloch(const fm_bloch_args *a) {
   FM_REQUIRE(a->n_pos >= 0, FM_ERR_SHAPE, "fm_bloch_solve_f32: negative n_pos");
   FM_REQUIRE(a->n_time >= 1, FM_ERR_SHAPE,
              "fm_bloch_solve_f32: rf_all must hold at least one sample (the initial state column)");
+  FM_REQUIRE(a->n_time <= INT32_MAX, FM_ERR_SHAPE, "fm_bloch_solve_f32: %lld time steps (at most 2^31 - 1)",
+             (long long)a->n_time);
   FM_REQUIRE((a->Mxy_hist == nullptr) == (a->Mz_hist == nullptr), FM_ERR_ARG,
              "fm_bloch_solve_f32: Mxy_hist and Mz_hist must be given together");
   if (a->n_pos > 0) {
@@ -295,7 +348,13 @@ int fm_bloch_solve_f32(fm_ctx *ctx, const fm_bloch_args *a, void *workspace, siz
         p.pod_term = k;
         r = md.terms[k].n_modes;
       }
-    if (n_pod == 0 || n_pod > 1 || r > 32) {
+    if (n_pod == 1 && md.n_terms == 1 && r <= 32) {
+      if (r <= 1) launch_bloch<4, 1>(p, hist, st);
+      else if (r <= 4) launch_bloch<4, 4>(p, hist, st);
+      else if (r <= 8) launch_bloch<4, 8>(p, hist, st);
+      else if (r <= 16) launch_bloch<4, 16>(p, hist, st);
+      else launch_bloch<4, 32>(p, hist, st);
+    } else if (n_pod == 0 || n_pod > 1 || r > 32) {
       launch_bloch<2, 0>(p, hist, st);
     } else if (r <= 1) {
       launch_bloch<1, 1>(p, hist, st);
