@@ -12,25 +12,41 @@
 
 namespace fm {
 
+// Step segments: runs of consecutive steps with the same dt and the same
+// RF-off state, so that the sweep tests neither per step.  seg[0] holds the
+// count G; seg[1 + g] the first step of segment g with the flags below;
+// seg[1 + G] the number of steps.
+constexpr int kSegNoRf = 1 << 30;  // rf = 0 on every step of the segment
+constexpr int kSegDt = 1 << 29;    // dt changes at the first step (e1, e2 recomputed)
+constexpr int kSegStep = kSegDt - 1;
+
 // Sequential pass over the steps: float32 running time (BlochSimulator.cpp:82-83),
-// the dt-changed flags (:72) and the motion call times.
+// the dt-changed flags (:72), the step segments and the motion call times.
 __global__ void bloch_prep_kernel(int64_t n_time, float gamma, const float2 *__restrict__ rf,
                                   const float *__restrict__ G, const float *__restrict__ dt, float4 *__restrict__ sa,
-                                  float4 *__restrict__ sb, int *__restrict__ changed, double *__restrict__ call_t) {
+                                  float4 *__restrict__ sb, int *__restrict__ seg, double *__restrict__ call_t) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   float ti = 0.0f, dti = -1.0f;
   const float mhg = __fmul_rn(-0.5f, gamma);
   if (call_t) call_t[0] = 0.0;
+  int n_seg = 0;
+  bool prev_norf = false;
   for (int64_t i = 0; i + 1 < n_time; ++i) {
     const float d = dt[i + 1];
-    changed[i] = (dti != d) ? 1 : 0;
+    const bool changed = dti != d;
     dti = d;
     ti = __fadd_rn(ti, dti);
     if (call_t) call_t[i + 1] = (double)ti;
     const float2 r = rf[i + 1];
     sa[i] = make_float4(r.x, r.y, __fmaf_rn(r.x, r.x, __fmul_rn(r.y, r.y)), __fmul_rn(mhg, dti));
     sb[i] = make_float4(G[3 * (i + 1) + 0], G[3 * (i + 1) + 1], G[3 * (i + 1) + 2], dti);
+    const bool norf = r.x == 0.f && r.y == 0.f;
+    if (i == 0 || changed || norf != prev_norf)
+      seg[1 + n_seg++] = (int)i | (norf ? kSegNoRf : 0) | (changed ? kSegDt : 0);
+    prev_norf = norf;
   }
+  seg[0] = n_seg;
+  seg[1 + n_seg] = (int)(n_time > 1 ? n_time - 1 : 0);
 }
 
 struct BlochDev {
@@ -40,7 +56,7 @@ struct BlochDev {
   const float2 *Mxy0;
   const float *Mz0;
   const float4 *sa, *sb;
-  const int *changed;
+  const int *seg;  // step segments (bloch_prep_kernel)
   MotionDev md;
   const float *weights;  // (n_time, slots) motion weights per call
   const float *table;    // TABLE motion: (n_time, N, 3)
@@ -87,27 +103,11 @@ __global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
     }
   }
 
-  float e1 = 0.f, e2 = 0.f;
-  // 32-bit step counter and running pointers (n_time < 2^31 is checked on
-  // the host): the per-step addressing is a few pointer increments.
-  const int steps = (int)(p.n_time - 1);
-  const float4 *sa = p.sa, *sb = p.sb;
-  const int *chg = p.changed;
-  const float *wrow = (MODE == 4) ? p.weights + p.md.slots + p.md.slot0[p.pod_term] : nullptr;
-  float2 *hist_m = HIST ? p.Mxy_hist + n : nullptr;
-  float *hist_z = HIST ? p.Mz_hist + n : nullptr;
-  for (int i = 0; i < steps; ++i, ++sa, ++sb, ++chg) {
-    const float4 a = *sa;
-    const float4 b = *sb;
-    if (HIST) {
-      hist_m += p.n;
-      hist_z += p.n;
-    }
-    if (*chg) {
-      e1 = expf(__fmul_rn(-b.w, invT1));
-      e2 = expf(__fmul_rn(-b.w, invT2));
-    }
-    float px = x, py = y, pz = z;
+  float e1 = 0.f, e2 = 0.f, rec = 0.f;  // rec = (1 - e1) M0, recomputed with e1
+
+  // Node position at the end of step i (i + 1 in the motion call times).
+  auto position = [&](int i, const float *wrow, float &px, float &py, float &pz) {
+    px = x; py = y; pz = z;
     if (MODE == 4) {
       // the single term's sum, as the k == 0 case of the term loop below
       float tx = 0.f, ty = 0.f, tz = 0.f;
@@ -118,7 +118,6 @@ __global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
         ty = fmaf(phy[m], wm, ty);
         tz = fmaf(phz[m], wm, tz);
       }
-      wrow += p.md.slots;
       px = __fadd_rn(x, tx); py = __fadd_rn(y, ty); pz = __fadd_rn(z, tz);
     } else if (MODE == 1 || MODE == 2) {
       const float *w = p.weights + (int64_t)(i + 1) * p.md.slots;
@@ -160,73 +159,120 @@ __global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
       const float *d = p.table + ((int64_t)(i + 1) * p.n + n) * 3;
       px = __fadd_rn(x, d[0]); py = __fadd_rn(y, d[1]); pz = __fadd_rn(z, d[2]);
     }
-    // Bz = r . G + dB  (BlochSimulator.cpp:104-107)
-    const float Bz = __fadd_rn(fmaf(pz, b.z, fmaf(py, b.y, __fmul_rn(px, b.x))), db);
-    if (a.x == 0.f && a.y == 0.f) {
-      // No RF on this step (the same for every thread): beta = 0, so the
-      // update reduces to Mxy' = conj(alpha)^2 Mxy, Mz' = |alpha|^2 Mz; the
-      // dropped terms of the general form below are exact zeros.  |rf|^2 is
-      // 0, and sqrt(RN(Bz^2)) = |Bz| exactly whenever Bz^2 is a normal float
-      // (checked for every float32 mantissa), so the norm needs no sqrt.
-      const float aBz = fabsf(Bz);
-      float Bn = (aBz >= 1e-18f && aBz <= 1e18f) ? aBz : sqrtf(__fmul_rn(Bz, Bz));
-      Bn = (Bn < 1e-12f) ? 1e-12f : Bn;
-      const float nz = __fmul_rn(Bz, __frcp_rn(Bn));
-      float s, c;
-      sincosf(__fmul_rn(Bn, a.w), &s, &c);
-      const float ca_i = nz * s;  // conj(alpha) = c + i nz s
-      const float a2 = fmaf(c, c, ca_i * ca_i);
-      const float ca2r = c * c - ca_i * ca_i, ca2i = 2.f * c * ca_i;
-      const float nmr = ca2r * mxy.x - ca2i * mxy.y;
-      const float nmi = ca2r * mxy.y + ca2i * mxy.x;
-      mxy.x = nmr * e2;
-      mxy.y = nmi * e2;
-      mz = fmaf(a2 * mz, e1, (1.f - e1) * M0);
-      if (HIST) {
-        *hist_m = mxy;
-        *hist_z = mz;
+  };
+
+  // Segments of steps with one dt and one RF-off state; inside a segment
+  // the loop has no per-step test.  32-bit step indices (n_time <= 2^29 is
+  // checked on the host) and running pointers.
+  const int n_seg = p.seg[0];
+  const int *segp = p.seg + 1;
+  for (int g = 0; g < n_seg; ++g) {
+    const int e0 = segp[g];
+    const int i0 = e0 & kSegStep, i1 = segp[g + 1] & kSegStep;
+    const float4 *sa = p.sa + i0, *sb = p.sb + i0;
+    const float *wrow = (MODE == 4) ? p.weights + (int64_t)(i0 + 1) * p.md.slots + p.md.slot0[p.pod_term] : nullptr;
+    float2 *hist_m = HIST ? p.Mxy_hist + (int64_t)(i0 + 1) * p.n + n : nullptr;
+    float *hist_z = HIST ? p.Mz_hist + (int64_t)(i0 + 1) * p.n + n : nullptr;
+    if (e0 & kSegDt) {
+      const float dtw = sb->w;
+      e1 = expf(__fmul_rn(-dtw, invT1));
+      rec = (1.f - e1) * M0;
+      e2 = expf(__fmul_rn(-dtw, invT2));
+    }
+    if (e0 & kSegNoRf) {
+      // No RF on these steps: beta = 0, so the update reduces to
+      // Mxy' = conj(alpha)^2 Mxy, Mz' = |alpha|^2 Mz; the dropped terms of
+      // the general form below are exact zeros.  |rf|^2 is 0, and
+      // max(sqrt(RN(Bz^2)), 1e-12) needs no sqrt below 1e18:
+      // sqrt(RN(Bz^2)) = |Bz| exactly whenever Bz^2 is a normal float
+      // (checked for every float32 mantissa), and below |Bz| = 1e-18 both
+      // forms clamp to 1e-12 (Bz = 0 on gradient-free steps included).
+      for (int i = i0; i < i1; ++i, ++sa, ++sb) {
+        const float aw = sa->w;
+        const float4 b = *sb;
+        float px, py, pz;
+        position(i, wrow, px, py, pz);
+        if (MODE == 4) wrow += p.md.slots;
+        // Bz = r . G + dB  (BlochSimulator.cpp:104-107)
+        const float Bz = __fadd_rn(fmaf(pz, b.z, fmaf(py, b.y, __fmul_rn(px, b.x))), db);
+        const float aBz = fabsf(Bz);
+        float Bn;
+        if (aBz <= 1e18f) {
+          Bn = (aBz < 1e-12f) ? 1e-12f : aBz;
+        } else {  // huge, infinite or NaN: the general form
+          Bn = sqrtf(__fmul_rn(Bz, Bz));
+          Bn = (Bn < 1e-12f) ? 1e-12f : Bn;
+        }
+        const float nz = __fmul_rn(Bz, __frcp_rn(Bn));
+        float s, c;
+        sincosf(__fmul_rn(Bn, aw), &s, &c);
+        const float ca_i = nz * s;  // conj(alpha) = c + i nz s
+        const float a2 = fmaf(c, c, ca_i * ca_i);
+        const float ca2r = c * c - ca_i * ca_i, ca2i = 2.f * c * ca_i;
+        const float nmr = ca2r * mxy.x - ca2i * mxy.y;
+        const float nmi = ca2r * mxy.y + ca2i * mxy.x;
+        mxy.x = nmr * e2;
+        mxy.y = nmi * e2;
+        mz = fmaf(a2 * mz, e1, rec);
+        if (HIST) {
+          *hist_m = mxy;
+          *hist_z = mz;
+          hist_m += p.n;
+          hist_z += p.n;
+        }
       }
       continue;
     }
-    float Bn = sqrtf(fmaf(Bz, Bz, a.z));
-    Bn = (Bn < 1e-12f) ? 1e-12f : Bn;
-    const float invB = __frcp_rn(Bn);
-    const float nz = __fmul_rn(Bz, invB);
-    const float hp = __fmul_rn(Bn, a.w);
-    float s, c;
-    sincosf(hp, &s, &c);
-    // alpha = c - i nz s ; beta = -i (rf/B) s   (BlochSimulator.cpp:114-126)
-    const float al_i = -nz * s;
-    const float nxr = __fmul_rn(a.x, invB), nxi = __fmul_rn(a.y, invB);
-    const float be_r = nxi * s, be_i = -nxr * s;
-    const float a2 = fmaf(c, c, al_i * al_i);
-    const float b2 = fmaf(be_r, be_r, be_i * be_i);
-    // conj(alpha) = c + i nz s  -> ca = (c, -al_i)
-    const float ca_r = c, ca_i = -al_i;
-    // 2 conj(a) beta Mz
-    const float t1r = 2.f * (ca_r * be_r - ca_i * be_i) * mz;
-    const float t1i = 2.f * (ca_r * be_i + ca_i * be_r) * mz;
-    // conj(a)^2 Mxy
-    const float ca2r = ca_r * ca_r - ca_i * ca_i, ca2i = 2.f * ca_r * ca_i;
-    const float t2r = ca2r * mxy.x - ca2i * mxy.y;
-    const float t2i = ca2r * mxy.y + ca2i * mxy.x;
-    // beta^2 conj(Mxy)
-    const float bb_r = be_r * be_r - be_i * be_i, bb_i = 2.f * be_r * be_i;
-    const float t3r = bb_r * mxy.x + bb_i * mxy.y;
-    const float t3i = bb_i * mxy.x - bb_r * mxy.y;
-    const float nmr = t1r + t2r - t3r;
-    const float nmi = t1i + t2i - t3i;
-    // Re(alpha beta conj(Mxy))
-    const float ab_r = c * be_r - al_i * be_i, ab_i = c * be_i + al_i * be_r;
-    const float re_abm = ab_r * mxy.x + ab_i * mxy.y;
-    const float nmz = (a2 - b2) * mz - 2.f * re_abm;
-    // relaxation (BlochSimulator.cpp:141-142)
-    mxy.x = nmr * e2;
-    mxy.y = nmi * e2;
-    mz = fmaf(nmz, e1, (1.f - e1) * M0);
-    if (HIST) {
-      *hist_m = mxy;
-      *hist_z = mz;
+    for (int i = i0; i < i1; ++i, ++sa, ++sb) {
+      const float4 a = *sa;
+      const float4 b = *sb;
+      float px, py, pz;
+      position(i, wrow, px, py, pz);
+      if (MODE == 4) wrow += p.md.slots;
+      // Bz = r . G + dB  (BlochSimulator.cpp:104-107)
+      const float Bz = __fadd_rn(fmaf(pz, b.z, fmaf(py, b.y, __fmul_rn(px, b.x))), db);
+      float Bn = sqrtf(fmaf(Bz, Bz, a.z));
+      Bn = (Bn < 1e-12f) ? 1e-12f : Bn;
+      const float invB = __frcp_rn(Bn);
+      const float nz = __fmul_rn(Bz, invB);
+      const float hp = __fmul_rn(Bn, a.w);
+      float s, c;
+      sincosf(hp, &s, &c);
+      // alpha = c - i nz s ; beta = -i (rf/B) s   (BlochSimulator.cpp:114-126)
+      const float al_i = -nz * s;
+      const float nxr = __fmul_rn(a.x, invB), nxi = __fmul_rn(a.y, invB);
+      const float be_r = nxi * s, be_i = -nxr * s;
+      const float a2 = fmaf(c, c, al_i * al_i);
+      const float b2 = fmaf(be_r, be_r, be_i * be_i);
+      // conj(alpha) = c + i nz s  -> ca = (c, -al_i)
+      const float ca_r = c, ca_i = -al_i;
+      // 2 conj(a) beta Mz
+      const float t1r = 2.f * (ca_r * be_r - ca_i * be_i) * mz;
+      const float t1i = 2.f * (ca_r * be_i + ca_i * be_r) * mz;
+      // conj(a)^2 Mxy
+      const float ca2r = ca_r * ca_r - ca_i * ca_i, ca2i = 2.f * ca_r * ca_i;
+      const float t2r = ca2r * mxy.x - ca2i * mxy.y;
+      const float t2i = ca2r * mxy.y + ca2i * mxy.x;
+      // beta^2 conj(Mxy)
+      const float bb_r = be_r * be_r - be_i * be_i, bb_i = 2.f * be_r * be_i;
+      const float t3r = bb_r * mxy.x + bb_i * mxy.y;
+      const float t3i = bb_i * mxy.x - bb_r * mxy.y;
+      const float nmr = t1r + t2r - t3r;
+      const float nmi = t1i + t2i - t3i;
+      // Re(alpha beta conj(Mxy))
+      const float ab_r = c * be_r - al_i * be_i, ab_i = c * be_i + al_i * be_r;
+      const float re_abm = ab_r * mxy.x + ab_i * mxy.y;
+      const float nmz = (a2 - b2) * mz - 2.f * re_abm;
+      // relaxation (BlochSimulator.cpp:141-142)
+      mxy.x = nmr * e2;
+      mxy.y = nmi * e2;
+      mz = fmaf(nmz, e1, rec);
+      if (HIST) {
+        *hist_m = mxy;
+        *hist_z = mz;
+        hist_m += p.n;
+        hist_z += p.n;
+      }
     }
   }
   if (p.Mxy_final) p.Mxy_final[n * p.final_stride] = mxy;
@@ -242,12 +288,12 @@ static void launch_bloch(const BlochDev &p, bool hist, cudaStream_t st) {
   else bloch_kernel<MODE, RMAX, false><<<blocks, threads, 0, st>>>(p);
 }
 
-static void carve_bloch(Carve &c, const fm_bloch_args *a, float4 **sa, float4 **sb, int **changed, double **call_t,
+static void carve_bloch(Carve &c, const fm_bloch_args *a, float4 **sa, float4 **sb, int **seg, double **call_t,
                         float **weights) {
   const int64_t steps = a->n_time > 1 ? a->n_time - 1 : 1;
   *sa = c.take<float4>(steps);
   *sb = c.take<float4>(steps);
-  *changed = c.take<int>(steps);
+  *seg = c.take<int>(steps + 2);
   *call_t = c.take<double>(a->n_time);
   *weights = c.take<float>((size_t)a->n_time * motion_slots(a->motion));
 }
@@ -257,7 +303,7 @@ static int validate_bloch(const fm_bloch_args *a) {
   FM_REQUIRE(a->n_pos >= 0, FM_ERR_SHAPE, "fm_bloch_solve_f32: negative n_pos");
   FM_REQUIRE(a->n_time >= 1, FM_ERR_SHAPE,
              "fm_bloch_solve_f32: rf_all must hold at least one sample (the initial state column)");
-  FM_REQUIRE(a->n_time <= INT32_MAX, FM_ERR_SHAPE, "fm_bloch_solve_f32: %lld time steps (at most 2^31 - 1)",
+  FM_REQUIRE(a->n_time <= (int64_t)kSegStep, FM_ERR_SHAPE, "fm_bloch_solve_f32: %lld time steps (at most 2^29 - 1)",
              (long long)a->n_time);
   FM_REQUIRE((a->Mxy_hist == nullptr) == (a->Mz_hist == nullptr), FM_ERR_ARG,
              "fm_bloch_solve_f32: Mxy_hist and Mz_hist must be given together");
@@ -301,16 +347,16 @@ int fm_bloch_solve_f32(fm_ctx *ctx, const fm_bloch_args *a, void *workspace, siz
   cudaStream_t st = ctx->stream;
   Carve cv(workspace, workspace_bytes);
   float4 *sa, *sb;
-  int *changed;
+  int *seg;
   double *call_t;
   float *weights;
-  carve_bloch(cv, a, &sa, &sb, &changed, &call_t, &weights);
+  carve_bloch(cv, a, &sa, &sb, &seg, &call_t, &weights);
   FM_TRY(carve_ok(cv, "fm_bloch_solve_f32"));
   if (a->n_pos == 0) return FM_OK;
 
   const MotionDev md = make_motion_dev(a->motion);
   bloch_prep_kernel<<<1, 1, 0, st>>>(a->n_time, a->gamma, reinterpret_cast<const float2 *>(a->rf), a->G, a->dt, sa,
-                                     sb, changed, md.kind == FM_MOTION_TERMS ? call_t : nullptr);
+                                     sb, seg, md.kind == FM_MOTION_TERMS ? call_t : nullptr);
   count_launch();
   FM_TRY(check_launch("bloch_prep_kernel"));
   FM_TRY(launch_motion_weights(md, call_t, a->n_time, weights, st));
@@ -322,7 +368,7 @@ int fm_bloch_solve_f32(fm_ctx *ctx, const fm_bloch_args *a, void *workspace, siz
   p.M0 = a->M0;
   p.Mxy0 = reinterpret_cast<const float2 *>(a->Mxy0);
   p.Mz0 = a->Mz0;
-  p.sa = sa; p.sb = sb; p.changed = changed;
+  p.sa = sa; p.sb = sb; p.seg = seg;
   p.md = md;
   p.weights = weights;
   p.table = (a->motion && a->motion->kind == FM_MOTION_TABLE) ? static_cast<const float *>(a->motion->table) : nullptr;
