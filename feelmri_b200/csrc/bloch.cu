@@ -8,6 +8,8 @@
 // ignored; e1/e2 are recomputed only when dt changes (BlochSimulator.cpp:69-99).
 #include <mutex>
 
+#include <math_constants.h>
+
 #include "motion.cuh"
 
 namespace fm {
@@ -183,10 +185,11 @@ __global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
       // No RF on these steps: beta = 0, so the update reduces to
       // Mxy' = conj(alpha)^2 Mxy, Mz' = |alpha|^2 Mz; the dropped terms of
       // the general form below are exact zeros.  |rf|^2 is 0, and
-      // max(sqrt(RN(Bz^2)), 1e-12) needs no sqrt below 1e18:
-      // sqrt(RN(Bz^2)) = |Bz| exactly whenever Bz^2 is a normal float
-      // (checked for every float32 mantissa), and below |Bz| = 1e-18 both
-      // forms clamp to 1e-12 (Bz = 0 on gradient-free steps included).
+      // clamp(sqrt(RN(Bz^2))) needs no sqrt: sqrt(RN(Bz^2)) = |Bz| exactly
+      // whenever Bz^2 is a normal float (checked for every float32
+      // mantissa); below |Bz| = 1e-18 both forms clamp to 1e-12 (Bz = 0 on
+      // gradient-free steps included); an overflowing square gives +inf and
+      // a NaN stays NaN in both.
       for (int i = i0; i < i1; ++i, ++sa, ++sb) {
         const float aw = sa->w;
         const float4 b = *sb;
@@ -195,14 +198,9 @@ __global__ void __launch_bounds__(128) bloch_kernel(BlochDev p) {
         if (MODE == 4) wrow += p.md.slots;
         // Bz = r . G + dB  (BlochSimulator.cpp:104-107)
         const float Bz = __fadd_rn(fmaf(pz, b.z, fmaf(py, b.y, __fmul_rn(px, b.x))), db);
-        const float aBz = fabsf(Bz);
-        float Bn;
-        if (aBz <= 1e18f) {
-          Bn = (aBz < 1e-12f) ? 1e-12f : aBz;
-        } else {  // huge, infinite or NaN: the general form
-          Bn = sqrtf(__fmul_rn(Bz, Bz));
-          Bn = (Bn < 1e-12f) ? 1e-12f : Bn;
-        }
+        const float sq = __fmul_rn(Bz, Bz);
+        float Bn = (sq == CUDART_INF_F) ? sq : fabsf(Bz);
+        Bn = (Bn < 1e-12f) ? 1e-12f : Bn;
         const float nz = __fmul_rn(Bz, __frcp_rn(Bn));
         float s, c;
         sincosf(__fmul_rn(Bn, aw), &s, &c);
