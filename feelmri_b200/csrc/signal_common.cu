@@ -137,6 +137,11 @@ int report_errors(Runs &r, cudaStream_t st, const char *who) {
   FM_REQUIRE(!(h & kErrTableCalls), FM_ERR_SHAPE,
              "%s: TABLE motion must hold one entry per distinct-time run of t", who);
   FM_REQUIRE(!(h & kErrTimeout), FM_ERR_TIMEOUT, "%s: a tensor-core pipeline wait timed out", who);
+  FM_REQUIRE(!(h & kErrPhaseRange), FM_ERR_ARG,
+             "%s: the split-BF16 form reduces phases k . r in fixed point and needs (|kx|+|ky|+|kz|) * "
+             "(|x|+|y|+|z|) below 2^27 cycles for every sample and moved node (or finite positions); use "
+             "precision f32 or f64",
+             who);
   return FM_OK;
 }
 

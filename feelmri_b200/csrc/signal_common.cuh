@@ -46,6 +46,7 @@ void carve_csr(Carve &c, int64_t rows, int64_t nnz, Csr &m);
 constexpr int kErrTimeout = 1;      // a tensor-core pipeline wait ran out
 constexpr int kErrSparseRow = 2;    // a row index of M outside [0, rows)
 constexpr int kErrTableCalls = 4;   // TABLE motion entries != distinct-time runs
+constexpr int kErrPhaseRange = 8;   // a tensor-core phase k . r may reach 2^27 cycles
 
 // Builds runs and tiles of `tile` samples on the device: counts[0] = runs,
 // counts[1] = tiles.  No host synchronisation.

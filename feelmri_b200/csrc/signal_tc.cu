@@ -16,8 +16,9 @@
 //   B'^T[(q,v,im)][2n..] = (Im B, Re B), so C'[p][2(q,v)+{0,1}] = (Re, Im).
 // * Split BF16.  Each operand x is stored as hi = bf16(x), lo = bf16(x - hi);
 //   hi*hi + hi*lo + lo*hi accumulate in FP32 in tensor memory.
-// * Phases.  k . r is evaluated in FP64 and reduced modulo one cycle before
-//   the FP32 sin/cos, so far nodes at high k keep their digits.
+// * Phases.  k . r is evaluated in FP64 and reduced modulo one cycle (in
+//   fixed point, to 2^-24 cycles) before the FP32 sin/cos, so far nodes at
+//   high k keep their digits.
 //
 // Block (persistent, one per SM): warps 0-7 produce operand tiles (16 nodes
 // per pipeline stage, 4 stages of shared memory in the UMMA no-swizzle
@@ -182,11 +183,17 @@ __device__ inline void split_pair(float a, float b, uint32_t &hi, uint32_t &lo) 
   lo = l;
 }
 
-// cos and sin of 2 pi c for c in cycles given in FP64: c is reduced modulo
-// one exactly (c - rint(c)) before the FP32 sin/cos.
+// cos and sin of 2 pi c for c in cycles given in FP64.  c is reduced modulo
+// one in fixed point: adding 1.5 * 2^29 leaves a double whose last place is
+// 2^-23, so its low 32 bits hold round(c * 2^23) modulo 2^32 and their low
+// 23 bits, sign-extended, are c - rint(c) in units of 2^-23 (error at most
+// 2^-24 cycles, for |c| < 2^28).  This keeps the reduction off the
+// transcendental unit (no rint, no double-to-float conversion): one FP64
+// add, two shifts and an integer-to-float conversion, then the FP32 sin/cos.
 __device__ inline void cycles_cos_sin(double c, float &co, float &s) {
-  const float f = __double2float_rn(__dsub_rn(c, rint(c)));
-  __sincosf(6.283185307179586f * f, &s, &co);
+  const int lo = __double2loint(__dadd_rn(c, 805306368.0));
+  const int frac = (lo << 9) >> 9;
+  __sincosf(__int2float_rn(frac) * 7.490140565847157e-07f, &s, &co);  // 2 pi / 2^23
 }
 
 __device__ inline void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
@@ -229,6 +236,12 @@ __device__ inline bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abo
   return false;
 }
 
+// Records |kx| + |ky| + |kz| of a phase row (float bits; a NaN counts as too large).
+__device__ inline void tc_note_k(int *kmax, double kx, double ky, double kz) {
+  const float s = (float)(fabs(kx) + fabs(ky) + fabs(kz));
+  atomicMax(kmax, __float_as_int(s) & 0x7fffffff);
+}
+
 __device__ inline void prefetch_l1(const void *ptr) { asm volatile("prefetch.global.L1 [%0];" ::"l"(ptr)); }
 
 // Raw node data loaded two stages before it is derived (global loads in
@@ -267,7 +280,7 @@ __device__ inline void tc_load_raw(const TcDev &p, int64_t n, TcRaw &r) {
 // off-resonance rotated weights W' = (M Mxy)[n, v] exp(-t / T2) exp(i phi t).
 // Nodes past the range get position 0 and zero weights, so they add nothing.
 __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, const TcRaw &r, const float *wrun,
-                                 double *pos, float2 *wblk, int slot) {
+                                 double *pos, float2 *wblk, int slot, int *rmax) {
   if (n < U.n_end) {
     float x = r.x, y = r.y, z = r.z;
     if (p.md.kind == FM_MOTION_TERMS) {
@@ -281,6 +294,8 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
     pos[slot] = (double)x;
     pos[kTcBlockNodes + slot] = (double)y;
     pos[2 * kTcBlockNodes + slot] = (double)z;
+    // |x| + |y| + |z| for the phase range check (a NaN counts as too large)
+    atomicMax(rmax, __float_as_int(fabsf(x) + fabsf(y) + fabsf(z)) & 0x7fffffff);
     // one weight set per run of the unit (stacked runs share positions)
     for (int k = 0; k < U.it.nrun; ++k) {
       const float tg = (float)p.run_t[U.it.run + k];
@@ -310,7 +325,7 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
 __device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, uint32_t blk, uint32_t j,
                                       TcRaw &raw, uint32_t &raw_seq, unsigned char *staging, uint64_t *rawfull,
                                       const float *wrun, double *pos_next, float2 *w_next,
-                                      volatile int *abort_flag) {
+                                      volatile int *abort_flag, int *rmax) {
   const int64_t n0 = U.n_begin + (int64_t)(blk + 1) * kTcBlockNodes;
   const int64_t n1 = n0 + tid;
   const bool staged = p.tma && n0 + kTcBlockNodes <= U.n_end;
@@ -347,7 +362,7 @@ __device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, 
       for (int v = 0; v < kTcVGroup; ++v)
         if (v < p.VG) raw.m[v] = sMM[tid * p.mm_ld + v];
     }
-    tc_derive(p, U, n1, raw, wrun, pos_next, w_next, tid);
+    tc_derive(p, U, n1, raw, wrun, pos_next, w_next, tid, rmax);
   }
 }
 
@@ -489,6 +504,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   uint64_t *rawfull = done + 1;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kTcMisc);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + kTcMisc + 4);
+  // largest |kx|+|ky|+|kz| of the unit's phases and |x|+|y|+|z| of its moved
+  // nodes (float bits), for the check that the fixed-point phase reduction
+  // applies (cycles_cos_sin)
+  int *kmax = reinterpret_cast<int *>(smem + kTcMisc + 8);
+  int *rmax = reinterpret_cast<int *>(smem + kTcMisc + 12);
   const uint32_t sbase = ptx::smem_addr(smem);
 
   if (tid == 0) {
@@ -497,6 +517,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     ptx::mbar_init(done, 1);
     ptx::mbar_init(rawfull, 1);
     *abort_flag = 0;
+    *kmax = 0;
+    *rmax = 0;
     ptx::fence_mbar_init();
   }
   if (warp == 0) ptx::tmem_alloc(tmem_slot, 2 * B.acc_cols);
@@ -563,6 +585,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         kx0 = p.kx[s_p];
         ky0 = p.ky[s_p];
         kz0 = p.kz[s_p];
+        if (nst > 0) tc_note_k(kmax, kx0, ky0, kz0);
       }
     } else {
       if (row < U.pairs) {
@@ -578,12 +601,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           kx0 = (double)p.kx[s_q] - (double)p.kx[s_0];
           ky0 = (double)p.ky[s_q] - (double)p.ky[s_0];
           kz0 = (double)p.kz[s_q] - (double)p.kz[s_0];
+          if (nst > 0) tc_note_k(kmax, kx0, ky0, kz0);
         }
         if (tq + 32 < U.Q_tile) {
           const int s_q = U.run.start + U.it.q0 + tq + 32;
           kx1 = (double)p.kx[s_q] - (double)p.kx[s_0];
           ky1 = (double)p.ky[s_q] - (double)p.ky[s_0];
           kz1 = (double)p.kz[s_q] - (double)p.kz[s_0];
+          if (nst > 0) tc_note_k(kmax, kx1, ky1, kz1);
         }
       }
     }
@@ -594,7 +619,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     if (loader && nst > 0) {
       const int64_t n = U.n_begin + tid;
       if (n < U.n_end) tc_load_raw(p, n, raw);
-      tc_derive(p, U, n, raw, wrun, pos_all, w_all, tid);
+      tc_derive(p, U, n, raw, wrun, pos_all, w_all, tid, rmax);
     }
     ptx::named_barrier(1, kTcProducers);  // block 0 is visible
     if (nst > 0) {
@@ -616,6 +641,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         gx = p.kx[s_p];
         gy = p.ky[s_p];
         gz = p.kz[s_p];
+        if (nst > 0) tc_note_k(kmax, gx, gy, gz);
       }
       const bool g_active = (warp & 3) * 32 < U.P_tile;
       const uint32_t ga0 = L.a_hi + kmajor_offset(grow, 8 * gc, kTcRows);
@@ -629,7 +655,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
         if (loader && blk + 1 < n_blocks && (j == 4 || j == 6))
           tc_stage_block(p, U, tid, blk, j, raw, raw_seq, smem + L.raw, rawfull, wrun,
-                         pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag);
+                         pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
+                         rmax);
         tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
         ptx::named_barrier(1, kTcProducers);
         if (issuer && st > 0)
@@ -679,7 +706,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         // (stages of block blk - 1) passed this block's first barrier.
         if (loader && blk + 1 < n_blocks && (j == 4 || j == 6))
           tc_stage_block(p, U, tid, blk, j, raw, raw_seq, smem + L.raw, rawfull, wrun,
-                         pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag);
+                         pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
+                         rmax);
         // wait until the MMAs that last read stage s are done
         tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
         // every writer of the previous stage is done (its MMAs go out now); the
@@ -787,6 +815,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     gst = g0 + nst;
     if (nst > 0) {
       ptx::named_barrier(1, kTcProducers);  // the unit's last stage is written
+      if (tid == 0) {
+        // every phase of the unit had |k . r| <= kmax rmax: the fixed-point
+        // reduction holds below 2^28 cycles (2^27 leaves a margin)
+        if (!((double)__int_as_float(*kmax) * (double)__int_as_float(*rmax) < 134217728.0))
+          atomicOr(p.error, kErrPhaseRange);
+        *kmax = 0;
+        *rmax = 0;
+      }
       if (issuer)
         tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, gst - 1, nst - 1, nst);
     }

@@ -149,3 +149,25 @@ def test_unstackable_runs_fall_back(cuda):
     K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
     err = fp64.rel_l2(K, _ref(M, traj, r0, phi, T2, Mxy))
     assert err < TOL, err
+
+
+@pytest.mark.parametrize("scale", [1.0, 1.0e8])
+def test_phase_range_is_checked(cuda, scale):
+    # the tensor-core form reduces k . r modulo one cycle in fixed point, which
+    # holds for (|kx|+|ky|+|kz|)(|x|+|y|+|z|) below 2^27 cycles: in range the
+    # result matches FP64, beyond it the call fails instead of returning wrong
+    # samples (|kx|+|ky|+|kz| up to ~140 1/m here; nodes scaled to ~1e7 m are
+    # far out of range)
+    from feelmri_b200._lib import FeelMRIError
+    mesh, N, M, Mxy, phi, T2 = _case(n=2000, V=1)
+    traj = W.cartesian(res=(8, 16, 4))
+    r0 = (mesh.nodes * scale).astype(np.float32)
+    if scale == 1.0:
+        K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+        assert fp64.rel_l2(K, _ref(M, traj, r0, phi, T2, Mxy)) < TOL
+    else:
+        with pytest.raises(FeelMRIError, match="2\\^27"):
+            Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+        # the context is still usable
+        K = Signal(0, M, traj.points, traj.t, mesh.nodes.astype(np.float32), phi, T2, Mxy, None, precision="bf16x3")
+        assert np.isfinite(K).all()
