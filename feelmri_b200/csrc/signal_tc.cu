@@ -236,24 +236,52 @@ __device__ inline bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abo
   return false;
 }
 
+// Shared-memory maximum of non-negative ints over the active lanes of a
+// warp: one atomic per warp instead of one per thread on the same address.
+__device__ inline void tc_note_max(int *dst, int v) {
+  const unsigned mask = __activemask();
+  const int m = __reduce_max_sync(mask, v);
+  if ((threadIdx.x & 31) == __ffs(mask) - 1) atomicMax(dst, m);
+}
+
 // Records |kx| + |ky| + |kz| of a phase row (float bits; a NaN counts as too large).
 __device__ inline void tc_note_k(int *kmax, double kx, double ky, double kz) {
   const float s = (float)(fabs(kx) + fabs(ky) + fabs(kz));
-  atomicMax(kmax, __float_as_int(s) & 0x7fffffff);
+  tc_note_max(kmax, __float_as_int(s) & 0x7fffffff);
 }
 
 __device__ inline void prefetch_l1(const void *ptr) { asm volatile("prefetch.global.L1 [%0];" ::"l"(ptr)); }
 
 // Raw node data loaded two stages before it is derived (global loads in
-// flight meanwhile); the node's POD mode rows are prefetched into L1 for the
-// displacement.
+// flight meanwhile).  With a single rank-1 POD term (the flow and respiratory
+// POD fits of the examples) the node's mode row is loaded into registers with
+// it; otherwise the mode rows are prefetched into L1 for the displacement.
+constexpr int kTcRegModes = 1;
 struct TcRaw {
   float x, y, z, t2, phi;
   float2 m[kTcVGroup];
+  float pmx[kTcRegModes], pmy[kTcRegModes], pmz[kTcRegModes];
 };
+// Mode count of the register-resident displacement, or -1 when the motion
+// is not a single POD term of at most kTcRegModes modes.
+__device__ inline int tc_reg_modes(const TcDev &p) {
+  return (p.md.kind == FM_MOTION_TERMS && p.md.n_terms == 1 && p.md.terms[0].kind != FM_TERM_RESPIRATORY &&
+          p.md.terms[0].n_modes <= kTcRegModes) ? p.md.terms[0].n_modes : -1;
+}
 
-__device__ inline void tc_prefetch_modes(const TcDev &p, int64_t n) {
+__device__ inline void tc_prefetch_modes(const TcDev &p, int64_t n, TcRaw &rr) {
   if (p.md.kind != FM_MOTION_TERMS) return;
+  const int rm = tc_reg_modes(p);
+  if (rm >= 0) {
+    const float *Phi = p.md.terms[0].modes + (size_t)n * 3 * rm;
+#pragma unroll
+    for (int m = 0; m < kTcRegModes; ++m) {
+      rr.pmx[m] = m < rm ? __ldg(Phi + m) : 0.f;
+      rr.pmy[m] = m < rm ? __ldg(Phi + rm + m) : 0.f;
+      rr.pmz[m] = m < rm ? __ldg(Phi + 2 * rm + m) : 0.f;
+    }
+    return;
+  }
   for (int k = 0; k < p.md.n_terms; ++k) {
     const fm_motion_term &T = p.md.terms[k];
     if (T.kind == FM_TERM_RESPIRATORY) continue;
@@ -272,7 +300,7 @@ __device__ inline void tc_load_raw(const TcDev &p, int64_t n, TcRaw &r) {
 #pragma unroll
   for (int v = 0; v < kTcVGroup; ++v)
     if (v < p.VG) r.m[v] = p.MM[n * p.mm_ld + v];
-  tc_prefetch_modes(p, n);
+  tc_prefetch_modes(p, n, r);
 }
 
 // Per-run node quantities of one node into slot `slot` of a node buffer:
@@ -283,7 +311,20 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
                                  double *pos, float2 *wblk, int slot, int *rmax) {
   if (n < U.n_end) {
     float x = r.x, y = r.y, z = r.z;
-    if (p.md.kind == FM_MOTION_TERMS) {
+    const int rm = tc_reg_modes(p);
+    if (rm >= 0) {
+      // motion_disp for one POD term, modes from registers (same arithmetic)
+      const float *wk = wrun + p.md.slot0[0];
+      float tx = 0.f, ty = 0.f, tz = 0.f;
+#pragma unroll
+      for (int m = 0; m < kTcRegModes; ++m) {
+        const float wm = m < rm ? wk[m] : 0.f;
+        tx = fmaf(r.pmx[m], wm, tx);
+        ty = fmaf(r.pmy[m], wm, ty);
+        tz = fmaf(r.pmz[m], wm, tz);
+      }
+      x = x + tx; y = y + ty; z = z + tz;
+    } else if (p.md.kind == FM_MOTION_TERMS) {
       float dx, dy, dz;
       motion_disp(p.md, wrun, n, p.N, dx, dy, dz);
       x = x + dx; y = y + dy; z = z + dz;
@@ -295,7 +336,7 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
     pos[kTcBlockNodes + slot] = (double)y;
     pos[2 * kTcBlockNodes + slot] = (double)z;
     // |x| + |y| + |z| for the phase range check (a NaN counts as too large)
-    atomicMax(rmax, __float_as_int(fabsf(x) + fabsf(y) + fabsf(z)) & 0x7fffffff);
+    tc_note_max(rmax, __float_as_int(fabsf(x) + fabsf(y) + fabsf(z)) & 0x7fffffff);
     // one weight set per run of the unit (stacked runs share positions)
     for (int k = 0; k < U.it.nrun; ++k) {
       const float tg = (float)p.run_t[U.it.run + k];
@@ -345,7 +386,7 @@ __device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, 
         ptx::bulk_copy_g2s(sphi, p.phi + n0, 4 * kTcBlockNodes, rawfull);
         ptx::bulk_copy_g2s(sMM, p.MM + n0 * p.mm_ld, 8 * kTcBlockNodes * p.mm_ld, rawfull);
       }
-      tc_prefetch_modes(p, n1);
+      tc_prefetch_modes(p, n1, raw);
     } else if (n1 < U.n_end) {
       tc_load_raw(p, n1, raw);
     }
