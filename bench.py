@@ -334,10 +334,10 @@ def run_e2e(args, case, w, precision) -> dict:
                    precision=precision if precision == "bf16x3" else None)
         return K
 
-    for _ in range(max(1, min(args.warmup, 2))):
+    for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
-    n = max(1, min(args.steps, 5))
+    n = max(5, min(args.steps, 20))
     t0 = time.perf_counter()
     for _ in range(n):
         K = step()
