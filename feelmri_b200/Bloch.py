@@ -20,6 +20,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+from . import _lib as L
 from . import ops
 from ._motion import lower, sample_table, table_motion
 from .BlochSimulator import bloch_call_times
@@ -159,6 +160,54 @@ class BlochSolver:
         out_z = torch.zeros((max(len(store), 1), N), dtype=torch.float32, device=dev)
         m = self._device_array("initial_Mxy")
         z = self._device_array("initial_Mz")
+        if blocks and lower(self.pod_trajectory, N, dev) is not None:
+            self._solve_sequence(blocks, store, r0, T1, T2, dB, m, z, out_m, out_z)
+        else:
+            self._solve_blocks(blocks, store, r0, T1, T2, dB, m, z, out_m, out_z)
+        for name, t in (("initial_Mxy", m), ("initial_Mz", z)):
+            if name in self._host:  # handed out: updated in place, as the reference does
+                host = self._host[name]
+                if host.ndim == 2:
+                    host[:, 0] = t.cpu().numpy()
+                else:
+                    host[...] = t.cpu().numpy().reshape(host.shape)
+        if not store:
+            return np.zeros((N, 0), np.complex64), np.zeros((N, 0), np.float32)
+        host_m, host_z = ops.to_host(out_m, out_z)
+        return host_m.T, host_z.T
+
+    def _solve_sequence(self, blocks, store, r0, T1, T2, dB, m, z, out_m, out_z):
+        """Every block in one sweep (fm_bloch_sequence_f32).  The motion is
+        lowered per block after update_timeshift(t0), as the block loop does;
+        the lowered descriptors differ only in their timeshifts."""
+        N = self.n_nodes
+        dev = self.device
+        seq, rfs, Gs, dts = [], [], [], []
+        motion = None
+        for i, block in enumerate(blocks):
+            times, rf, G, t0 = discretise(block)
+            if self.pod_trajectory is not None:
+                self.pod_trajectory.update_timeshift(t0)
+            mo = lower(self.pod_trajectory, N, dev)
+            if mo is None:  # a callable whose state no longer lowers: run block by block
+                return self._solve_blocks(blocks, store, r0, T1, T2, dB, m, z, out_m, out_z)
+            motion = mo
+            shifts = tuple((mo.struct.terms[k].timeshift, mo.struct.terms[k].timeshift_kind)
+                           for k in range(mo.struct.n_terms)) if mo.struct.kind == L.FM_MOTION_TERMS else ()
+            seq.append(ops.SequenceBlock(n_time=times.shape[0], empty=bool(getattr(block, "empty", False)),
+                                         store=store.index(i) if i in store else -1, timeshifts=shifts))
+            rfs.append(rf)
+            Gs.append(np.ascontiguousarray(G, np.float32).reshape(-1, 3))
+            dts.append(np.diff(times, prepend=0).astype(np.float32))
+        up = lambda a, dt=None: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        ops.bloch_sequence(r0, T1, T2, dB, self.M0, self.gamma, seq, up(np.concatenate(rfs).astype(np.complex64)),
+                           up(np.concatenate(Gs)), up(np.concatenate(dts)), m, z, motion, out_m, out_z,
+                           Mxy_carry=m, Mz_carry=z)
+
+    def _solve_blocks(self, blocks, store, r0, T1, T2, dB, m, z, out_m, out_z):
+        """Block by block (a motion that is sampled on the host)."""
+        N = self.n_nodes
+        dev = self.device
         for i, block in enumerate(blocks):
             times, rf, G, t0 = discretise(block)
             if self.pod_trajectory is not None:
@@ -183,14 +232,3 @@ class BlochSolver:
                 z.copy_(fin_z)
                 if empty:
                     m.copy_(fin_m)
-        for name, t in (("initial_Mxy", m), ("initial_Mz", z)):
-            if name in self._host:  # handed out: updated in place, as the reference does
-                host = self._host[name]
-                if host.ndim == 2:
-                    host[:, 0] = t.cpu().numpy()
-                else:
-                    host[...] = t.cpu().numpy().reshape(host.shape)
-        if not store:
-            return np.zeros((N, 0), np.complex64), np.zeros((N, 0), np.float32)
-        host_m, host_z = ops.to_host(out_m, out_z)
-        return host_m.T, host_z.T

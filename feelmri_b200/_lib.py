@@ -98,6 +98,43 @@ class BlochArgs(C.Structure):
     ]
 
 
+class BlochBlock(C.Structure):
+    _fields_ = [
+        ("offset", _i64),
+        ("n_time", _i64),
+        ("empty", C.c_int32),
+        ("store", C.c_int32),
+        ("timeshift", C.c_double * FM_MAX_MOTION_TERMS),
+        ("timeshift_kind", C.c_int32 * FM_MAX_MOTION_TERMS),
+    ]
+
+
+class BlochSequenceArgs(C.Structure):
+    _fields_ = [
+        ("n_pos", _i64),
+        ("r0", _p),
+        ("T1", _p),
+        ("T2", _p),
+        ("delta_B", _p),
+        ("M0", C.c_float),
+        ("gamma", C.c_float),
+        ("n_blocks", C.c_int32),
+        ("blocks", C.POINTER(BlochBlock)),
+        ("n_samples", _i64),
+        ("rf", _p),
+        ("G", _p),
+        ("dt", _p),
+        ("Mxy0", _p),
+        ("Mz0", _p),
+        ("motion", C.POINTER(Motion)),
+        ("n_store", C.c_int32),
+        ("Mxy_out", _p),
+        ("Mz_out", _p),
+        ("Mxy_carry", _p),
+        ("Mz_carry", _p),
+    ]
+
+
 class SignalArgs(C.Structure):
     _fields_ = [
         ("n_nodes", _i64),
@@ -162,6 +199,8 @@ SIGNATURES = {
     "fm_bloch_solve_f32": (C.c_int, [_p, C.POINTER(BlochArgs), _p, C.c_size_t]),
     "fm_bloch_workspace_size": (C.c_int, [C.POINTER(BlochArgs), C.POINTER(C.c_size_t)]),
     "fm_bloch_solve_f32_noalloc": (C.c_int, [_p, C.POINTER(BlochArgs)]),
+    "fm_bloch_sequence_f32": (C.c_int, [_p, C.POINTER(BlochSequenceArgs), _p, C.c_size_t]),
+    "fm_bloch_sequence_workspace_size": (C.c_int, [C.POINTER(BlochSequenceArgs), C.POINTER(C.c_size_t)]),
     "fm_signal": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, _p, C.c_size_t]),
     "fm_signal_enqueue": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, _p, C.c_size_t]),
     "fm_signal_status": (C.c_int, [_p, C.POINTER(SignalArgs), C.c_int, _p, C.c_size_t]),

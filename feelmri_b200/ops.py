@@ -189,6 +189,67 @@ def bloch_solve(inp: BlochInputs, motion: LoweredMotion, history: bool = True,
     return Mxy_final, Mz_final
 
 
+@dataclass
+class SequenceBlock:
+    """One block of a device-side block sequence (fm_bloch_sequence_f32)."""
+    n_time: int
+    empty: bool = False
+    store: int = -1                    # row of the stored final states, or -1
+    timeshifts: tuple = ()             # ((value, FM_NUM_* kind), ...) per motion term
+
+
+def bloch_sequence(r0: torch.Tensor, T1: torch.Tensor, T2: torch.Tensor, delta_B: torch.Tensor, M0: float,
+                   gamma: float, blocks: list[SequenceBlock], rf: torch.Tensor, G: torch.Tensor, dt: torch.Tensor,
+                   Mxy0: torch.Tensor, Mz0: torch.Tensor, motion: LoweredMotion, Mxy_out: torch.Tensor,
+                   Mz_out: torch.Tensor, Mxy_carry: torch.Tensor | None = None,
+                   Mz_carry: torch.Tensor | None = None) -> None:
+    """Runs a whole block sequence in one sweep: rf / G / dt hold the blocks'
+    samples concatenated in block order; block i's final state goes to row
+    blocks[i].store of Mxy_out / Mz_out when that is >= 0; the state carried
+    past the last block goes to Mxy_carry / Mz_carry (which may alias Mxy0 /
+    Mz0).  motion is NONE or TERMS (the per-block timeshifts replace its
+    terms')."""
+    dev = r0.device
+    N = r0.shape[0]
+    S = rf.shape[0]
+    _check_dev("r0", r0, torch.float32, (N, 3), dev)
+    for name, t in (("T1", T1), ("T2", T2), ("delta_B", delta_B), ("Mz0", Mz0)):
+        _check_dev(name, t, torch.float32, (N,), dev)
+    _check_dev("Mxy0", Mxy0, torch.complex64, (N,), dev)
+    _check_dev("rf", rf, torch.complex64, (S,), dev)
+    _check_dev("G", G, torch.float32, (S, 3), dev)
+    _check_dev("dt", dt, torch.float32, (S,), dev)
+    n_store = Mxy_out.shape[0]
+    _check_dev("Mxy_out", Mxy_out, torch.complex64, (n_store, N), dev)
+    _check_dev("Mz_out", Mz_out, torch.float32, (n_store, N), dev)
+    if Mxy_carry is not None:
+        _check_dev("Mxy_carry", Mxy_carry, torch.complex64, (N,), dev)
+    if Mz_carry is not None:
+        _check_dev("Mz_carry", Mz_carry, torch.float32, (N,), dev)
+    table = (L.BlochBlock * max(len(blocks), 1))()
+    off = 0
+    for i, b in enumerate(blocks):
+        e = table[i]
+        e.offset, e.n_time, e.empty, e.store = off, int(b.n_time), int(bool(b.empty)), int(b.store)
+        for k, (v, kind) in enumerate(b.timeshifts):
+            e.timeshift[k], e.timeshift_kind[k] = float(v), int(kind)
+        off += int(b.n_time)
+    a = L.BlochSequenceArgs()
+    a.n_pos = N
+    a.r0, a.T1, a.T2, a.delta_B = _ptr(r0), _ptr(T1), _ptr(T2), _ptr(delta_B)
+    a.M0, a.gamma = float(np.float32(M0)), float(np.float32(gamma))
+    a.n_blocks, a.blocks, a.n_samples = len(blocks), table, S
+    a.rf, a.G, a.dt = _ptr(rf), _ptr(G), _ptr(dt)
+    a.Mxy0, a.Mz0 = _ptr(Mxy0), _ptr(Mz0)
+    a.motion = C.pointer(motion.struct)
+    a.n_store, a.Mxy_out, a.Mz_out = n_store, _ptr(Mxy_out), _ptr(Mz_out)
+    a.Mxy_carry, a.Mz_carry = _ptr(Mxy_carry), _ptr(Mz_carry)
+    nbytes = C.c_size_t()
+    L.check(L.lib().fm_bloch_sequence_workspace_size(C.byref(a), C.byref(nbytes)))
+    ws = workspace(dev, nbytes.value)
+    L.check(L.lib().fm_bloch_sequence_f32(ctx_for(dev), C.byref(a), ws.data_ptr(), ws.numel()))
+
+
 # ----------------------------------------------------------------- Signal --
 
 @dataclass

@@ -190,6 +190,62 @@ FM_API int fm_bloch_solve_f32(fm_ctx *ctx, const fm_bloch_args *args, void *work
                        size_t workspace_bytes);
 FM_API int fm_bloch_workspace_size(const fm_bloch_args *args, size_t *bytes);
 
+/* ---- BlochSolver.solve: a whole block sequence in one sweep ------------- */
+/* One block of a sequence (host array). */
+typedef struct fm_bloch_block {
+  int64_t offset;          /* first sample of the block in rf / G / dt      */
+  int64_t n_time;          /* samples of the block (>= 1); the first sample
+                              is the block's initial-state column            */
+  int32_t empty;           /* nonzero: the final Mxy is carried on; zero:
+                              0 * Mxy is carried (Bloch.py:363-367)          */
+  int32_t store;           /* row of Mxy_out / Mz_out for the block's final
+                              state (store_magnetization), or -1            */
+  double timeshift[FM_MAX_MOTION_TERMS];       /* each motion term's .timeshift
+                              during the block (update_timeshift(t0))       */
+  int32_t timeshift_kind[FM_MAX_MOTION_TERMS]; /* FM_NUM_* of those values   */
+} fm_bloch_block;
+
+typedef struct fm_bloch_sequence_args {
+  int64_t n_pos;           /* N                                             */
+  const float *r0;         /* (N, 3) row-major                              */
+  const float *T1, *T2;    /* (N,) ms                                       */
+  const float *delta_B;    /* (N,) mT                                       */
+  float M0;
+  float gamma;             /* rad / (ms mT)                                 */
+  int32_t n_blocks;
+  const fm_bloch_block *blocks; /* host array of n_blocks, offsets contiguous
+                              from 0 in block order                          */
+  int64_t n_samples;       /* sum of the blocks' n_time                     */
+  const float *rf;         /* (n_samples,) complex64, mT, blocks concatenated */
+  const float *G;          /* (n_samples, 3) row-major, mT/m                 */
+  const float *dt;         /* (n_samples,) ms; each block's first is ignored */
+  const float *Mxy0;       /* (N,) complex64 state before the first block   */
+  const float *Mz0;        /* (N,)                                          */
+  const fm_motion *motion; /* NULL, NONE or TERMS (a TABLE motion is not
+                              accepted); the per-block timeshifts replace
+                              terms[k].timeshift                             */
+  int32_t n_store;         /* rows of Mxy_out / Mz_out                      */
+  float *Mxy_out;          /* (n_store, N) complex64 stored final states    */
+  float *Mz_out;           /* (n_store, N) float32                          */
+  float *Mxy_carry;        /* (N,) state carried past the last block, or
+                              NULL; may alias Mxy0                          */
+  float *Mz_carry;         /* (N,) or NULL; may alias Mz0                   */
+} fm_bloch_sequence_args;
+
+/* Replaces BlochSolver.solve's block loop (python/feelmri/Bloch.py:332-368),
+ * which calls solve_mri (cpp/feelmri/BlochSimulator.cpp:12-148 / :151-277)
+ * once per block and carries the state on the host: here every block runs in
+ * one sweep with the magnetisation in registers.  Per block: the motion
+ * terms' timeshift is the block's, each block's dt[0] is ignored and its
+ * running time restarts at 0; after the block its final state is stored when
+ * requested and 0 * Mxy is carried on unless the block is empty.  Stored rows
+ * and the carried state equal the per-block fm_bloch_solve_f32 loop's bit for
+ * bit.  The block table is copied to the device from host memory, so this
+ * call is not meant for stream capture. */
+FM_API int fm_bloch_sequence_f32(fm_ctx *ctx, const fm_bloch_sequence_args *args, void *workspace,
+                                 size_t workspace_bytes);
+FM_API int fm_bloch_sequence_workspace_size(const fm_bloch_sequence_args *args, size_t *bytes);
+
 /* Scratch held by the library for fm_bloch_solve_f32_noalloc, per device. */
 #define FM_NOALLOC_BLOCH_SCRATCH_BYTES (4u << 20)
 

@@ -60,6 +60,9 @@ STRUCTS = {
     "fm_signal_args": (L.SignalArgs, ["n_nodes", "m_nnz", "m_data", "kx", "Mxy", "motion", "out"]),
     "fm_mass_args": (L.MassArgs, ["n_elems", "nodes_per_elem", "elems", "n_qpoints", "tabulated"]),
     "fm_tc_tuning": (L.TcTuning, ["split_nodes", "kz_cap", "reserved"]),
+    "fm_bloch_block": (L.BlochBlock, ["offset", "n_time", "empty", "store", "timeshift", "timeshift_kind"]),
+    "fm_bloch_sequence_args": (L.BlochSequenceArgs, ["n_pos", "M0", "gamma", "n_blocks", "blocks", "n_samples",
+                                                     "rf", "motion", "n_store", "Mxy_out", "Mz_carry"]),
 }
 
 

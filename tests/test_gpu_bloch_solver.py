@@ -116,3 +116,52 @@ def test_state_arrays_follow_the_reference(cuda):
     m2, z2 = t.solve(start=-1)
     np.testing.assert_array_equal(m1, m2)
     np.testing.assert_array_equal(z1, z2)
+
+
+def _mixed_blocks():
+    """Blocks of different lengths, dt changes, empty gaps and stored states."""
+    blocks = []
+    t = 0.0
+    for i in range(5):
+        b = W.hard_pulse_block(t, 15.0 + 5 * i, 3.0 + i, grad=((1.0, -2.0, 0.5), 0.4, 0.8),
+                               store=(i in (1, 4)), dt=0.05 if i % 2 else 0.1)
+        blocks.append(b)
+        t += 3.0 + i
+        gap = W.hard_pulse_block(t, 0.0, 1.5)
+        gap.empty = True
+        gap.store_magnetization = (i == 2)
+        blocks.append(gap)
+        t += 1.5
+    return blocks
+
+
+@pytest.mark.parametrize("motion", ["none", "pod", "pod_sum"])
+def test_sequence_sweep_equals_block_loop(cuda, motion):
+    # the whole sequence in one launch (fm_bloch_sequence_f32) against the
+    # per-block solves with the state carried between them: same bits
+    mesh = W.cylinder(3000)
+    N = mesh.n_nodes
+    T1, T2 = W.tissue(N)
+    nodes = mesh.nodes.astype(np.float32)
+    dB = np.random.default_rng(2).normal(0, 1e-4, N).astype(np.float32)
+
+    def make_pod():
+        if motion == "none":
+            return None
+        p = W.sinusoidal_pod(N, n_modes=3, amp=1e-3, period=9.0, n_frames=7)
+        if motion == "pod_sum":
+            from feelmri_b200.Motion import PODSum
+            p = PODSum(p, W.sinusoidal_pod(N, n_modes=2, amp=5e-4, period=5.0, n_frames=5, seed=9))
+        return p
+
+    results = []
+    for path in ("sequence", "blocks"):
+        s = BlochSolver(_mixed_blocks(), nodes, M0=1.0, T1=T1, T2=T2, delta_B=dB, gamma=W.GAMMA,
+                        pod_trajectory=make_pod())
+        if path == "blocks":
+            s._solve_sequence = s._solve_blocks
+        m, z = s.solve()
+        results.append((m, z, s.initial_Mxy.copy(), s.initial_Mz.copy()))
+    for a, b in zip(*results):
+        np.testing.assert_array_equal(a, b)
+    assert results[0][0].shape == (N, 3)
