@@ -22,7 +22,7 @@ import torch
 
 from . import _lib as L
 from . import ops
-from ._motion import lower, sample_table, table_motion
+from ._motion import lower, sample_table, table_motion, term_timeshifts
 from .BlochSimulator import bloch_call_times
 
 __all__ = ["BlochSolver", "discretise"]
@@ -188,12 +188,16 @@ class BlochSolver:
             times, rf, G, t0 = discretise(block)
             if self.pod_trajectory is not None:
                 self.pod_trajectory.update_timeshift(t0)
-            mo = lower(self.pod_trajectory, N, dev)
-            if mo is None:  # a callable whose state no longer lowers: run block by block
-                return self._solve_blocks(blocks, store, r0, T1, T2, dB, m, z, out_m, out_z)
-            motion = mo
-            shifts = tuple((mo.struct.terms[k].timeshift, mo.struct.terms[k].timeshift_kind)
-                           for k in range(mo.struct.n_terms)) if mo.struct.kind == L.FM_MOTION_TERMS else ()
+            if motion is None:
+                motion = lower(self.pod_trajectory, N, dev)
+                if motion is None:  # the callable no longer lowers: run block by block
+                    return self._solve_blocks(blocks, store, r0, T1, T2, dB, m, z, out_m, out_z)
+            shifts = ()
+            if motion.struct.kind == L.FM_MOTION_TERMS:
+                ts = term_timeshifts(self.pod_trajectory)
+                if ts is None or len(ts) != motion.struct.n_terms:
+                    return self._solve_blocks(blocks, store, r0, T1, T2, dB, m, z, out_m, out_z)
+                shifts = tuple(ts)
             seq.append(ops.SequenceBlock(n_time=times.shape[0], empty=bool(getattr(block, "empty", False)),
                                          store=store.index(i) if i in store else -1, timeshifts=shifts))
             rfs.append(rf)

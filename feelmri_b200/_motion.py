@@ -214,6 +214,24 @@ def _single(obj, device):
     return _pod_term(obj, device) or _respiratory_term(obj, device)
 
 
+def term_timeshifts(obj) -> list | None:
+    """(value, FM_NUM_* kind) of each term's .timeshift, in the order lower()
+    lays the terms out (a left-nested PODSum left to right); None when a
+    timeshift has a type lower() would refuse.  Reads only the timeshifts, so
+    a block sequence can follow update_timeshift() without lowering again."""
+    if any(k.__name__ == "PODSum" for k in type(obj).__mro__) and _defined_by(obj, "__call__", {"PODSum"}):
+        left = term_timeshifts(obj.pod1)
+        right = term_timeshifts(obj.pod2)
+        if left is None or right is None or len(right) != 1:
+            return None
+        return left + right
+    ts = getattr(obj, "timeshift", 0.0)
+    kind = num_kind(ts)
+    if kind in (None, L.FM_NUM_NONE):
+        return None
+    return [(float(np.asarray(ts, dtype=np.float64)), kind)]
+
+
 def lower(pod_trajectory, n_nodes: int, device: torch.device) -> LoweredMotion | None:
     """Returns the device descriptor of a motion callable, or None when the
     callable is not one this module can lower (the caller then samples it)."""

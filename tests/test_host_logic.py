@@ -151,3 +151,22 @@ def test_lil_conversion_declines_what_scipy_must_handle():
     z[0, 0] = 1 + 2j
     got = pb.sparse_csc(z, np.float32)
     np.testing.assert_array_equal(got[3], np.array([1.0], np.float32))
+
+
+def test_term_timeshifts_follow_the_lowering():
+    # the block-sequence sweep reads each block's timeshifts without lowering
+    # again; they must be exactly what lower() would put in the descriptor
+    from feelmri_b200._motion import lower, term_timeshifts
+    from feelmri_b200.Motion import PODSum
+    N = 50
+    a = W.sinusoidal_pod(N, n_modes=2, n_frames=5)
+    b = W.sinusoidal_pod(N, n_modes=1, n_frames=5, seed=3)
+    c = W.sinusoidal_pod(N, n_modes=3, n_frames=6, seed=4)
+    for obj in (a, PODSum(a, b), PODSum(PODSum(a, b), c)):
+        for t0 in (0.0, np.float32(2.5), np.float64(7.25), 3):
+            obj.update_timeshift(t0)
+            low = lower(obj, N, torch.device("cpu"))
+            got = term_timeshifts(obj)
+            want = [(low.struct.terms[k].timeshift, low.struct.terms[k].timeshift_kind)
+                    for k in range(low.struct.n_terms)]
+            assert got == want
