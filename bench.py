@@ -834,6 +834,47 @@ def run_sequence(args) -> dict:
             "bit_identical_to_block_loop": bool(same)}
 
 
+def run_pod_build(args) -> dict:
+    """POD construction (Motion.POD) from displacement snapshots at the
+    precision workload's scale: 500k nodes x 3 components x 40 frames,
+    rank-10 fit.  numpy (the reference's computation) against
+    backend="cuda" (snapshot products on the GPU), both end to end from host
+    arrays, host clock."""
+    import torch
+    from feelmri_b200.Motion import POD
+    rng = np.random.default_rng(6)
+    P, t, r = args.nodes if args.nodes != N_NODES else 500_000, 40, 10
+    times = np.linspace(0.0, 800.0, t)
+    modes = rng.normal(0.0, 1e-3, (P, 3, r)).astype(np.float32)
+    # distinct frequencies and decaying amplitudes: a well-separated rank-10 history
+    freq, amp = np.arange(1, r + 1), 0.8 ** np.arange(r)
+    w = (amp * np.sin(2 * np.pi * freq[None, :] * times[:, None] / 800.0 + rng.uniform(0, 6, r)[None, :])).astype(
+        np.float32)
+    data = np.einsum("pcm,tm->pct", modes, w).astype(np.float32)
+    torch.cuda.init()
+    POD(times[:4], data[:1000, :, :4], n_modes=2, backend="cuda")  # load the library, warm the context
+    out = {}
+    for backend in ("cuda", "numpy"):
+        ts = []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            pod = POD(times, data, n_modes=r, backend=backend)
+            ts.append(time.perf_counter() - t0)
+        out[backend] = {"s": statistics.median(ts), "modes": pod.modes, "weights": pod.weights}
+    errs = []
+    for m in range(r):
+        a, b = out["numpy"]["modes"][..., m], out["cuda"]["modes"][..., m]
+        sgn = np.sign(np.vdot(a.ravel(), b.ravel()))
+        errs.append(float(np.linalg.norm(a - sgn * b) / np.linalg.norm(a)))
+    return {"metric": "POD construction time (Motion.POD, rank 10)", "value": out["cuda"]["s"], "unit": "s",
+            "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": out["cuda"]["s"] * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 data, f64 sums",
+            "data": "synthetic rank-10 displacement snapshots",
+            "config": {"workload": f"POD of {P} nodes x 3 x {t} frames, {r} modes", "timer": "host wall clock"},
+            "numpy_s": out["numpy"]["s"], "speedup_vs_numpy": out["numpy"]["s"] / out["cuda"]["s"],
+            "max_mode_rel_diff_vs_numpy": max(errs)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -845,7 +886,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--workload", default="phase_contrast",
-                    choices=["phase_contrast", "batching", "serving", "precision", "sequence"],
+                    choices=["phase_contrast", "batching", "serving", "precision", "sequence", "pod"],
                     help="phase_contrast: the metric's configuration; batching: many phantoms in one launch; "
                          "serving: a Poisson request stream; precision: radial, 8 coils, rank-10 motion")
     ap.add_argument("--requests", type=int, default=24)
@@ -869,6 +910,8 @@ def main():
         res = run_precision(args)
     elif args.workload == "sequence":
         res = run_sequence(args)
+    elif args.workload == "pod":
+        res = run_pod_build(args)
     else:
         res = run_gpu(args)
     if res is not None:

@@ -80,7 +80,14 @@ class POD:
     """Snapshot POD of nodal vectors (P, C, t) with spline-interpolated weights."""
 
     def __init__(self, times, data, global_to_local=None, n_modes=5, is_periodic=False,
-                 interpolation_method="Pchip", timeshift=0.0):
+                 interpolation_method="Pchip", timeshift=0.0, *, backend="numpy"):
+        """backend="cuda" forms the snapshot products (X^T X, X E, X^T phi)
+        on the GPU (fm_pod_gram_*, fm_pod_project_*) with FP64 sums; the
+        t x t eigenproblem and the spline fit stay on the host as in the
+        reference.  The default "numpy" is the reference's computation."""
+        if backend not in ("numpy", "cuda"):
+            raise ValueError(f"backend must be 'numpy' or 'cuda'; got {backend!r}")
+        self.backend = backend
         self.times = times
         self.data = data
         self.local_to_global_map = global_to_local
@@ -118,12 +125,24 @@ class POD:
         flat = self.data.reshape(-1, n_t)
         if remove_mean:
             flat = flat - np.mean(flat, axis=1, keepdims=True)
-        cov = flat.T @ flat
+        device = self.backend == "cuda" and flat.dtype in (np.float32, np.float64)
+        if device:
+            import torch
+            from . import ops
+            X = torch.from_numpy(np.ascontiguousarray(flat)).to(ops.require_cuda())
+            cov = ops.pod_gram(X).cpu().numpy().astype(flat.dtype)
+        else:
+            cov = flat.T @ flat
         vals, vecs = np.linalg.eigh(cov)
         order = np.argsort(vals)[::-1][: self.n_modes]
         vals, vecs = vals[order], vecs[:, order]
-        phi = flat @ (vecs / np.sqrt(vals).reshape(1, -1))
-        weights = np.einsum("pn, pt -> nt", flat, phi)
+        E = vecs / np.sqrt(vals).reshape(1, -1)
+        if device:
+            phi_d, w_d = ops.pod_project(X, torch.from_numpy(np.ascontiguousarray(E, np.float64)).to(X.device))
+            phi, weights = phi_d.cpu().numpy(), w_d.cpu().numpy().astype(flat.dtype)
+        else:
+            phi = flat @ E
+            weights = np.einsum("pn, pt -> nt", flat, phi)
         phi = phi.reshape((self.data.shape[0], -1, self.n_modes))
         if self.local_to_global_map is not None:
             phi = phi[self.local_to_global_map, :, :]

@@ -193,6 +193,11 @@ SIGNATURES = {
     "fm_ctx_timing_query": (C.c_int, [_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "fm_pod_tensordot_f32": (C.c_int, [_p, _p, _p, _i64, _i64, _i64, _p]),
     "fm_pod_tensordot_f64": (C.c_int, [_p, _p, _p, _i64, _i64, _i64, _p]),
+    "fm_pod_build_workspace_size": (C.c_int, [_i64, C.c_int32, C.c_int32, C.POINTER(C.c_size_t)]),
+    "fm_pod_gram_f32": (C.c_int, [_p, _p, _i64, C.c_int32, _p, _p, C.c_size_t]),
+    "fm_pod_gram_f64": (C.c_int, [_p, _p, _i64, C.c_int32, _p, _p, C.c_size_t]),
+    "fm_pod_project_f32": (C.c_int, [_p, _p, _i64, C.c_int32, _p, C.c_int32, _p, _p, _p, C.c_size_t]),
+    "fm_pod_project_f64": (C.c_int, [_p, _p, _i64, C.c_int32, _p, C.c_int32, _p, _p, _p, C.c_size_t]),
     "fm_coil_expand": (C.c_int, [_p, _p, _p, _i64, _i64, _p]),
     "fm_motion_eval": (C.c_int, [_p, C.POINTER(Motion), _i64, _p, _i64, _p, _p, C.c_size_t]),
     "fm_motion_eval_workspace_size": (C.c_int, [C.POINTER(Motion), _i64, _i64, C.POINTER(C.c_size_t)]),

@@ -17,6 +17,7 @@ BUILD = ROOT / "_build"
 SOURCES = [
     "context.cu",
     "pod.cu",
+    "pod_build.cu",
     "bloch.cu",
     "signal_common.cu",
     "signal_plain.cu",

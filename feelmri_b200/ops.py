@@ -103,6 +103,39 @@ def tensordot_modes_weights(modes: torch.Tensor, weights: torch.Tensor, out: tor
     return out
 
 
+def _pod_ws(rows: int, t: int, r: int, dev) -> torch.Tensor:
+    nbytes = C.c_size_t()
+    L.check(L.lib().fm_pod_build_workspace_size(rows, t, r, C.byref(nbytes)))
+    return workspace(dev, nbytes.value)
+
+
+def pod_gram(X: torch.Tensor) -> torch.Tensor:
+    """X^T X (t x t, float64) of a (rows, t) float32/float64 snapshot matrix."""
+    if X.dim() != 2 or X.dtype not in (torch.float32, torch.float64) or not X.is_contiguous():
+        raise ValueError("pod_gram: X must be a contiguous (rows, t) float32/float64 tensor")
+    rows, t = X.shape
+    out = torch.empty((t, t), dtype=torch.float64, device=X.device)
+    ws = _pod_ws(rows, t, 0, X.device)
+    fn = L.lib().fm_pod_gram_f32 if X.dtype == torch.float32 else L.lib().fm_pod_gram_f64
+    L.check(fn(ctx_for(X.device), X.data_ptr(), rows, t, out.data_ptr(), ws.data_ptr(), ws.numel()))
+    return out
+
+
+def pod_project(X: torch.Tensor, E: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor]:
+    """phi = X E (rows x r, X's type) and weights = X^T phi (t x r, float64)."""
+    rows, t = X.shape
+    if E.dtype != torch.float64 or E.shape[0] != t or E.dim() != 2 or not E.is_contiguous():
+        raise ValueError("pod_project: E must be a contiguous (t, r) float64 tensor")
+    r = E.shape[1]
+    phi = torch.empty((rows, r), dtype=X.dtype, device=X.device)
+    weights = torch.empty((t, r), dtype=torch.float64, device=X.device)
+    ws = _pod_ws(rows, t, r, X.device)
+    fn = L.lib().fm_pod_project_f32 if X.dtype == torch.float32 else L.lib().fm_pod_project_f64
+    L.check(fn(ctx_for(X.device), X.data_ptr(), rows, t, E.data_ptr(), r, phi.data_ptr(), weights.data_ptr(),
+               ws.data_ptr(), ws.numel()))
+    return phi, weights
+
+
 def motion_eval(motion: LoweredMotion, n_nodes: int, times, device: torch.device) -> torch.Tensor:
     """Displacements (len(times), N, 3) of a lowered motion at host times."""
     times = np.ascontiguousarray(times, dtype=np.float64)

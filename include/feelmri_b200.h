@@ -136,6 +136,28 @@ FM_API int fm_pod_tensordot_f64(fm_ctx *ctx, const double *modes,
                          const double *weights, int64_t P, int64_t C,
                          int64_t M, double *out);
 
+/* Snapshot products of POD.calculate_pod (python/feelmri/Motion.py:174-211),
+ * the O(rows t^2) part of building a POD, on the device.  X is the
+ * (rows x t) snapshot matrix data.reshape(-1, t) (rows = P * C), row-major.
+ *   fm_pod_gram_*:    gram = X^T X, (t x t) float64            (Motion.py:189)
+ *   fm_pod_project_*: phi = X E (rows x n_modes, X's type) and
+ *                     weights = X^T phi (t x n_modes, float64)   (Motion.py:202-204)
+ * with E (t x n_modes, float64) the scaled eigenvectors; the t x t
+ * eigenproblem stays on the host.  Sums are accumulated in FP64 in a fixed
+ * order (reproducible run to run); 1 <= t <= 1024.  All pointers are device
+ * memory; the workspace is sized by fm_pod_build_workspace_size.  New
+ * component: the reference builds the POD with numpy on the host. */
+FM_API int fm_pod_build_workspace_size(int64_t rows, int32_t t, int32_t n_modes, size_t *bytes);
+FM_API int fm_pod_gram_f32(fm_ctx *ctx, const float *X, int64_t rows, int32_t t, double *gram, void *workspace,
+                           size_t workspace_bytes);
+FM_API int fm_pod_gram_f64(fm_ctx *ctx, const double *X, int64_t rows, int32_t t, double *gram, void *workspace,
+                           size_t workspace_bytes);
+FM_API int fm_pod_project_f32(fm_ctx *ctx, const float *X, int64_t rows, int32_t t, const double *E,
+                              int32_t n_modes, float *phi, double *weights, void *workspace, size_t workspace_bytes);
+FM_API int fm_pod_project_f64(fm_ctx *ctx, const double *X, int64_t rows, int32_t t, const double *E,
+                              int32_t n_modes, double *phi, double *weights, void *workspace,
+                              size_t workspace_bytes);
+
 /* Evaluates a lowered motion callable at n_times host-given times, exactly as
  * pod_trajectory(t) would (python/feelmri/Motion.py:237-254, :272-290,
  * :303-309, :58-103): out (n_times, N, 3) float32.  `times` is a HOST array

@@ -161,3 +161,35 @@ def test_motion_golden_device_displacements(cuda):
         disp = ops.motion_eval(low, gold.shape[1], d[f"{name}/t"], dev).cpu().numpy()
         scale = np.nanmax(np.abs(gold)) if np.isfinite(gold).any() else 1.0
         np.testing.assert_allclose(disp, gold, rtol=1e-5, atol=2e-7 * scale, equal_nan=True, err_msg=name)
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.float32, 2e-4), (np.float64, 1e-9)])
+def test_pod_construction_on_device(cuda, dtype, tol):
+    # Motion.POD(backend="cuda"): the snapshot products on the GPU, the t x t
+    # eigenproblem on the host; modes, weights and the evaluated motion match
+    # the numpy construction (eigenvector signs are arbitrary: aligned first)
+    from feelmri_b200.Motion import POD
+    rng = np.random.default_rng(11)
+    P, t, r_true = 6000, 24, 4
+    times = np.linspace(0.0, 100.0, t)
+    base = rng.normal(size=(P, 3, r_true))
+    amp = np.array([3.0, 1.5, 0.7, 0.3])
+    freq = np.arange(1, r_true + 1)  # distinct frequencies: a well-separated rank-4 history
+    w = np.sin(2 * np.pi * freq[None, :] * times[:, None] / 100.0 + rng.uniform(0, 6, r_true)[None, :]) * amp
+    data = (np.einsum("pcm,tm->pct", base, w) + 1e-4 * rng.normal(size=(P, 3, t))).astype(dtype)
+    ref = POD(times, data, n_modes=3)
+    dev = POD(times, data, n_modes=3, backend="cuda")
+    assert dev.modes.dtype == ref.modes.dtype and dev.weights.dtype == ref.weights.dtype
+    for m in range(3):
+        s = np.sign(np.vdot(ref.modes[..., m].ravel(), dev.modes[..., m].ravel()))
+        dm = dev.modes[..., m] * s
+        dw = dev.weights[:, m] * s
+        assert np.linalg.norm(dm - ref.modes[..., m]) / np.linalg.norm(ref.modes[..., m]) < tol
+        assert np.linalg.norm(dw - ref.weights[:, m]) / np.linalg.norm(ref.weights[:, m]) < tol
+    # the motion itself does not depend on the signs
+    for tq in (0.0, 37.5, 99.0):
+        a, b = ref(tq), dev(tq)
+        assert np.linalg.norm(a - b) / np.linalg.norm(a) < tol
+    # reproducible: FP64 sums in a fixed order
+    again = POD(times, data, n_modes=3, backend="cuda")
+    np.testing.assert_array_equal(again.modes, dev.modes)
