@@ -55,7 +55,14 @@ constexpr int kTcVGroup = 8;        // Mxy columns per launch
 // number of MMAs added into one accumulator; 32 stages (512 nodes, 192 MMAs)
 // keep it near 1e-5.
 constexpr int kTcDrain = 32;
+// Stages a generic (unfactored, N = 16) unit writes between two barriers.  At
+// most kTcStages: a group's stages must use distinct ring slots, whose
+// previous MMAs went out at an earlier barrier (so no wait can depend on the
+// group's own MMAs).
+constexpr int kTcGenGroup = 4;
 constexpr uint64_t kTcWaitNs = 2000000000ull;
+static_assert(kTcGenGroup <= kTcStages && kTcStagesPerBlock % kTcGenGroup == 0 && kTcDrain % kTcGenGroup == 0,
+              "generic stage groups must fit the ring, the node blocks and the accumulation groups");
 constexpr uint32_t kAStageBytes = kTcRows * 2 * kTcNodes * 2;  // 128 rows x 32 K x bf16 = 8 KB
 
 struct TcRun {
@@ -691,47 +698,59 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       const bool g_b = tid < kTcRows && gpair < NH;
       const int gv = gpair < VG ? gpair : 0;
       const uint32_t gbr = kmajor_offset(gpair, 2 * gnode, NT), gbi = kmajor_offset(NH + gpair, 2 * gnode, NT);
-      for (uint32_t st = 0; st < nst; ++st) {
-        const uint32_t g = g0 + st, s = g & (kTcStages - 1);
-        const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
-        if (loader && blk + 1 < n_blocks && (j == 4 || j == 6))
-          tc_stage_block(p, U, tid, blk, j, raw, raw_seq, smem + L.raw, rawfull, wrun,
-                         pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
-                         rmax);
-        tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
-        ptx::named_barrier(1, kTcProducers);
-        if (issuer && st > 0)
-          tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g - 1, st - 1, nst);
-        const uint32_t stg = sstages + s * L.stage_bytes;
-        if (g_active) {
-          const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 4 * gc;
-          uint32_t h[4], l[4];
+      // The MMAs of a generic stage are small (N = 16), so the producers
+      // write kTcGenGroup stages between barriers and the issuer sends them
+      // together: one barrier per group instead of one per stage.  Groups
+      // divide the 8-stage node blocks, so a block derived at stage 6 is
+      // visible after its group's barrier, before any stage of it is read.
+      for (uint32_t sg = 0; sg < nst; sg += kTcGenGroup) {
+        const uint32_t s_end = min(nst, sg + (uint32_t)kTcGenGroup);
+        for (uint32_t st = sg; st < s_end; ++st) {
+          const uint32_t g = g0 + st, s = g & (kTcStages - 1);
+          const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
+          if (loader && blk + 1 < n_blocks && (j == 4 || j == 6))
+            tc_stage_block(p, U, tid, blk, j, raw, raw_seq, smem + L.raw, rawfull, wrun,
+                           pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
+                           rmax);
+          // the MMAs that last read stage s were sent at an earlier barrier
+          tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
+          const uint32_t stg = sstages + s * L.stage_bytes;
+          if (g_active) {
+            const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 4 * gc;
+            uint32_t h[4], l[4];
 #pragma unroll
-          for (int u4 = 0; u4 < 4; u4 += 2) {
-            const double2 x = *reinterpret_cast<const double2 *>(px + u4);
-            const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
-            const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
-            float c0, s0, c1, s1;
-            cycles_cos_sin(fma(gz, z.x, fma(gy, y.x, gx * x.x)), c0, s0);
-            cycles_cos_sin(fma(gz, z.y, fma(gy, y.y, gx * x.y)), c1, s1);
-            split_pair(c0, s0, h[u4], l[u4]);
-            split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
+            for (int u4 = 0; u4 < 4; u4 += 2) {
+              const double2 x = *reinterpret_cast<const double2 *>(px + u4);
+              const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
+              const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
+              float c0, s0, c1, s1;
+              cycles_cos_sin(fma(gz, z.x, fma(gy, y.x, gx * x.x)), c0, s0);
+              cycles_cos_sin(fma(gz, z.y, fma(gy, y.y, gx * x.y)), c1, s1);
+              split_pair(c0, s0, h[u4], l[u4]);
+              split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
+            }
+            st_shared_v4(stg + ga0, h[0], h[1], h[2], h[3]);
+            st_shared_v4(stg + gl0, l[0], l[1], l[2], l[3]);
           }
-          st_shared_v4(stg + ga0, h[0], h[1], h[2], h[3]);
-          st_shared_v4(stg + gl0, l[0], l[1], l[2], l[3]);
-        }
-        if (g_b) {
-          const float2 wv = w_all[(buf * WR + gv) * kWStride + j * kTcNodes + gnode];
-          uint32_t hb, lb;
-          split_pair(wv.x, wv.y, hb, lb);
-          const uint32_t hm = __byte_perm(hb, 0u, 0x1032) ^ 0x80000000u, lm = __byte_perm(lb, 0u, 0x1032) ^ 0x80000000u;
-          asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_hi + gbr), "r"(hb));
-          asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_lo + gbr), "r"(lb));
-          asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_hi + gbi), "r"(hm));
-          asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_lo + gbi), "r"(lm));
+          if (g_b) {
+            const float2 wv = w_all[(buf * WR + gv) * kWStride + j * kTcNodes + gnode];
+            uint32_t hb, lb;
+            split_pair(wv.x, wv.y, hb, lb);
+            const uint32_t hm = __byte_perm(hb, 0u, 0x1032) ^ 0x80000000u, lm = __byte_perm(lb, 0u, 0x1032) ^ 0x80000000u;
+            asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_hi + gbr), "r"(hb));
+            asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_lo + gbr), "r"(lb));
+            asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_hi + gbi), "r"(hm));
+            asm volatile("st.shared.b32 [%0], %1;" ::"r"(stg + L.b_lo + gbi), "r"(lm));
+          }
         }
         ptx::fence_proxy_async_smem();
-        if ((st & (kTcDrain - 1)) == 0 && st > 0) {
+        // every writer of the group is done: its MMAs go out now
+        ptx::named_barrier(1, kTcProducers);
+        if (issuer)
+          for (uint32_t st = sg; st < s_end; ++st) tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst);
+        // an accumulation group ended with this group: fold it before the
+        // next group's MMAs (which go out at the next barrier)
+        if (s_end < nst && (s_end & (kTcDrain - 1)) == 0) {
           tc_fold(p, B.acc_cols, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
@@ -864,7 +883,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         *kmax = 0;
         *rmax = 0;
       }
-      if (issuer)
+      if (issuer && fac)  // generic groups went out at their own barriers
         tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, gst - 1, nst - 1, nst);
     }
     if (U.n_groups > 0) tc_final(p, B.acc_cols, W, U, accfull, tmem, gbase + U.n_groups - 1, U.n_groups > 1, abort_flag);
