@@ -9,6 +9,10 @@ for the GPU forms (relative L2 errors are stated against it).
   'exact'.  Vectorised over samples in chunks: identical mathematics, node sums
   by numpy's pairwise summation.
 * lumped_p1(): exact P1 lumped weights (vol / 4 per element vertex).
+* nudft_adjoint(): the exact adjoint NUDFT as a direct sum, the check of the
+  GPU reconstruction operators (feelmri_b200.Recon); the reference's own
+  reconstruction uses pynufft's gridding approximation (not installed here),
+  against which the GPU operators are unpinned.
 """
 from __future__ import annotations
 
@@ -107,6 +111,23 @@ def signal(M, kx, ky, kz, t, r0, phi, T2, Mxy, disp=None, pi_mode="exact", sampl
             out[order[b0 + c0:b0 + c0 + ii.size]] = E @ W
     if sample_idx is None:
         return out.reshape(*grid, V)
+    return out
+
+
+def nudft_adjoint(kx, ky, kz, kdata, points, dcw=None, pi_mode="float", chunk=512):
+    """Float64 exact adjoint NUDFT I[n, c] = sum_s w_s K[s, c] exp(+i 2 pi k_s . x_n)
+    at `points` (n, 3); the direct sum, independent of the Signal restatement.
+    The GPU reconstruction (feelmri_b200.Recon) uses the Signal's float pi."""
+    two_pi = 2.0 * (np.pi if pi_mode == "exact" else FLOAT_PI)
+    k = np.stack([np.asarray(a, np.float64).reshape(-1) for a in (kx, ky, kz)], axis=1)
+    K = np.asarray(kdata, np.complex128).reshape(k.shape[0], -1)
+    if dcw is not None:
+        K = K * np.asarray(dcw, np.float64).reshape(-1, 1)
+    x = np.asarray(points, np.float64).reshape(-1, 3)
+    out = np.zeros((x.shape[0], K.shape[1]), np.complex128)
+    for c0 in range(0, x.shape[0], chunk):
+        E = np.exp(1j * two_pi * (x[c0:c0 + chunk] @ k.T))
+        out[c0:c0 + chunk] = E @ K
     return out
 
 

@@ -170,3 +170,24 @@ def test_term_timeshifts_follow_the_lowering():
             want = [(low.struct.terms[k].timeshift, low.struct.terms[k].timeshift_kind)
                     for k in range(low.struct.n_terms)]
             assert got == want
+
+
+def test_recon_grid_and_analytic_weights():
+    # voxel centres on the DFT-centred grid; the analytic density weights of
+    # Recon.py:108-146 restated (ramp for radials, readout speed for spirals)
+    from feelmri_b200 import Recon
+    X, Y, Z = Recon.grid_points((4, 5, 1), (0.08, 0.1, 0.01))
+    np.testing.assert_allclose(X[:, 0, 0], np.array([-2, -1, 0, 1]) * 0.02, atol=1e-7)
+    np.testing.assert_allclose(Y[0, :, 0], np.array([-2, -1, 0, 1, 2]) * 0.02, atol=1e-7)
+    assert np.all(Z == 0)
+    R, L, S = 6, 4, 2
+    rng = np.random.default_rng(0)
+    kx, ky, kz = (rng.normal(size=(R, L, S)) for _ in range(3))
+    w = Recon.dcf_radial_stack(kx, ky)
+    r = np.sqrt(kx ** 2 + ky ** 2)
+    np.testing.assert_allclose(w, (r / (r.mean(axis=(0, 1), keepdims=True) + 1e-6)).ravel(), rtol=1e-6)
+    ws = Recon.dcf_local_speed_readout(kx, ky, kz).reshape(R, L, S)
+    dk = np.sqrt(np.diff(kx, axis=0) ** 2 + np.diff(ky, axis=0) ** 2 + np.diff(kz, axis=0) ** 2)
+    mid = 0.5 * (dk[:-1] + dk[1:])
+    full = np.concatenate([dk[:1], mid, dk[-1:]], axis=0)
+    np.testing.assert_allclose(ws, full / (full.mean(axis=0, keepdims=True) + 1e-8), rtol=1e-5)
