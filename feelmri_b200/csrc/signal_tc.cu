@@ -60,9 +60,17 @@ constexpr int kTcDrain = 32;
 // previous MMAs went out at an earlier barrier (so no wait can depend on the
 // group's own MMAs).
 constexpr int kTcGenGroup = 4;
+// Stages a factored unit writes between two barriers.  The B warps compute
+// the phase table of stage st + kTcFacGroup during stage st, so the table
+// ring holds 2 kTcFacGroup buffers (kTcEBufs).
+constexpr int kTcFacGroup = 2;
+constexpr int kTcEBufs = 2 * kTcFacGroup;
 constexpr uint64_t kTcWaitNs = 2000000000ull;
 static_assert(kTcGenGroup <= kTcStages && kTcStagesPerBlock % kTcGenGroup == 0 && kTcDrain % kTcGenGroup == 0,
               "generic stage groups must fit the ring, the node blocks and the accumulation groups");
+static_assert(kTcFacGroup <= kTcStages && kTcStagesPerBlock % kTcFacGroup == 0 && kTcDrain % kTcFacGroup == 0 &&
+                  (kTcEBufs & (kTcEBufs - 1)) == 0 && kTcFacGroup <= 2,
+              "factored stage groups: the node block is requested at stage 2 and derived at stage 4 of 8");
 constexpr uint32_t kAStageBytes = kTcRows * 2 * kTcNodes * 2;  // 128 rows x 32 K x bf16 = 8 KB
 
 struct TcRun {
@@ -158,8 +166,8 @@ __host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
   off += 2 * 3 * kTcBlockNodes * 8;
   L.w = off;  // [2][VG][kWStride] float2
   off += 2 * VG * kWStride * 8;
-  L.etab = off;  // [2][Qt][kEStride] float2, by stage parity
-  off += 2 * Qt * kEStride * 8;
+  L.etab = off;  // [kTcEBufs][Qt][kEStride] float2, by stage
+  off += kTcEBufs * Qt * kEStride * 8;
   L.raw = off;  // staging of one raw node block (bulk copies), when used
   L.total = off;
   return L;
@@ -365,12 +373,12 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
   }
 }
 
-// Node block blk + 1 of a unit, at stage j of block blk (threads 0-127, one
-// node each).  j == 4: a full block with p.tma is requested by bulk copies
-// into the staging area (thread 0; completion on rawfull), any other block by
-// register loads.  j == 6: the block is derived into the other node buffer.
-// raw_seq counts the staged blocks (the rawfull phase).
-__device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, uint32_t blk, uint32_t j,
+// Node block blk + 1 of a unit (threads 0-127, one node each), in two calls
+// some stages apart.  request: a full block with p.tma is requested by bulk
+// copies into the staging area (thread 0; completion on rawfull), any other
+// block by register loads.  Otherwise the block is derived into the other
+// node buffer.  raw_seq counts the staged blocks (the rawfull phase).
+__device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, uint32_t blk, bool request,
                                       TcRaw &raw, uint32_t &raw_seq, unsigned char *staging, uint64_t *rawfull,
                                       const float *wrun, double *pos_next, float2 *w_next,
                                       volatile int *abort_flag, int *rmax) {
@@ -381,7 +389,7 @@ __device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, 
   float *sT2 = sr0 + 3 * kTcBlockNodes;
   float *sphi = sT2 + kTcBlockNodes;
   float2 *sMM = reinterpret_cast<float2 *>(sphi + kTcBlockNodes);
-  if (j == 4) {
+  if (request) {
     if (staged) {
       if (tid == 0) {
         // the staging area's previous readers (the last block's derive) are
@@ -670,9 +678,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       tc_derive(p, U, n, raw, wrun, pos_all, w_all, tid, rmax);
     }
     ptx::named_barrier(1, kTcProducers);  // block 0 is visible
-    if (nst > 0) {
-      if (t_on0) tc_phase_pair(pos_all, etab, tq, tn, kx0, ky0, kz0);
-      if (t_on1) tc_phase_pair(pos_all, etab, tq + 32, tn, kx1, ky1, kz1);
+    // phase tables of the first group's stages (block 0, buffers 0 ..)
+    for (uint32_t st = 0; st < kTcFacGroup && st < nst; ++st) {
+      float2 *et = etab + st * Qt * kEStride;
+      if (t_on0) tc_phase_pair(pos_all + st * kTcNodes, et, tq, tn, kx0, ky0, kz0);
+      if (t_on1) tc_phase_pair(pos_all + st * kTcNodes, et, tq + 32, tn, kx1, ky1, kz1);
     }
     const uint32_t g0 = gst;
     int next_drain = 0;
@@ -709,7 +719,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           const uint32_t g = g0 + st, s = g & (kTcStages - 1);
           const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
           if (loader && blk + 1 < n_blocks && (j == 4 || j == 6))
-            tc_stage_block(p, U, tid, blk, j, raw, raw_seq, smem + L.raw, rawfull, wrun,
+            tc_stage_block(p, U, tid, blk, j == 4, raw, raw_seq, smem + L.raw, rawfull, wrun,
                            pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
                            rmax);
           // the MMAs that last read stage s were sent at an earlier barrier
@@ -757,116 +767,126 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       }
     } else if (a_role) {
       // ------------------------------------------------------- A rows --
+      // kTcFacGroup stages between barriers; the group's MMAs go out at its
+      // barrier.  Node block blk + 1 is requested at j == 2 and derived at
+      // j == 4 into the other buffer: that buffer's readers (block blk - 1)
+      // are done, and the phase tables of block blk + 1's first stages are
+      // computed after the barrier that ends the derive's group.
       const bool active = (rw >> 1) * 32 < U.rows;
-      for (uint32_t st = 0; st < nst; ++st) {
-        const uint32_t g = g0 + st, s = g & (kTcStages - 1);
-        const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
-        // block blk + 1 (block blk is then complete): requested at j == 4,
-        // derived into the other buffer at j == 6.  That buffer's readers
-        // (stages of block blk - 1) passed this block's first barrier.
-        if (loader && blk + 1 < n_blocks && (j == 4 || j == 6))
-          tc_stage_block(p, U, tid, blk, j, raw, raw_seq, smem + L.raw, rawfull, wrun,
-                         pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
-                         rmax);
-        // wait until the MMAs that last read stage s are done
-        tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
-        // every writer of the previous stage is done (its MMAs go out now); the
-        // phase table of this stage and the node blocks derived up to the
-        // previous stage are visible
-        ptx::named_barrier(1, kTcProducers);
-        if (issuer && st > 0)
-          tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g - 1, st - 1, nst);
-        if (active) {
-          // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n
-          const uint32_t stg = sstages + s * L.stage_bytes;
-          const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 8 * half;
-          uint32_t h[8], l[8];
+      for (uint32_t sg = 0; sg < nst; sg += kTcFacGroup) {
+        const uint32_t s_end = min(nst, sg + (uint32_t)kTcFacGroup);
+        for (uint32_t st = sg; st < s_end; ++st) {
+          const uint32_t g = g0 + st, s = g & (kTcStages - 1);
+          const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
+          if (loader && blk + 1 < n_blocks && (j == 2 || j == 4))
+            tc_stage_block(p, U, tid, blk, j == 2, raw, raw_seq, smem + L.raw, rawfull, wrun,
+                           pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
+                           rmax);
+          // wait until the MMAs that last read stage s are done (sent at an
+          // earlier barrier)
+          tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
+          if (active) {
+            // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n
+            const uint32_t stg = sstages + s * L.stage_bytes;
+            const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 8 * half;
+            uint32_t h[8], l[8];
 #pragma unroll
-          for (int u4 = 0; u4 < 8; u4 += 2) {
-            const double2 x = *reinterpret_cast<const double2 *>(px + u4);
-            const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
-            const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
-            float c0, s0, c1, s1;
-            cycles_cos_sin(fma(kz0, z.x, fma(ky0, y.x, kx0 * x.x)), c0, s0);
-            cycles_cos_sin(fma(kz0, z.y, fma(ky0, y.y, kx0 * x.y)), c1, s1);
-            split_pair(c0, s0, h[u4], l[u4]);
-            split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
+            for (int u4 = 0; u4 < 8; u4 += 2) {
+              const double2 x = *reinterpret_cast<const double2 *>(px + u4);
+              const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
+              const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
+              float c0, s0, c1, s1;
+              cycles_cos_sin(fma(kz0, z.x, fma(ky0, y.x, kx0 * x.x)), c0, s0);
+              cycles_cos_sin(fma(kz0, z.y, fma(ky0, y.y, kx0 * x.y)), c1, s1);
+              split_pair(c0, s0, h[u4], l[u4]);
+              split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
+            }
+            const uint32_t a_st = stg + o_hi;
+            st_shared_v4(a_st, h[0], h[1], h[2], h[3]);
+            st_shared_v4(a_st + 128, h[4], h[5], h[6], h[7]);
+            st_shared_v4(a_st + d_lo, l[0], l[1], l[2], l[3]);
+            st_shared_v4(a_st + d_lo + 128, l[4], l[5], l[6], l[7]);
           }
-          const uint32_t a_st = stg + o_hi;
-          st_shared_v4(a_st, h[0], h[1], h[2], h[3]);
-          st_shared_v4(a_st + 128, h[4], h[5], h[6], h[7]);
-          st_shared_v4(a_st + d_lo, l[0], l[1], l[2], l[3]);
-          st_shared_v4(a_st + d_lo + 128, l[4], l[5], l[6], l[7]);
         }
         ptx::fence_proxy_async_smem();
-        // the previous group's last MMAs went out at this stage's barrier:
-        // fold the accumulator into the running sum before the next group
-        // starts (its first MMAs go out at the next stage's barrier)
-        if ((st & (kTcDrain - 1)) == 0 && st > 0) {
+        // every writer of the group is done (and its phase tables of the next
+        // group are visible after this barrier): its MMAs go out now
+        ptx::named_barrier(1, kTcProducers);
+        if (issuer)
+          for (uint32_t st = sg; st < s_end; ++st) tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst);
+        // an accumulation group ended with this group: fold it before the
+        // next group's MMAs go out
+        if (s_end < nst && (s_end & (kTcDrain - 1)) == 0) {
           tc_fold(p, B.acc_cols, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
       }
     } else {
       // ------------------------------------------------------- B rows --
-      for (uint32_t st = 0; st < nst; ++st) {
-        const uint32_t g = g0 + st, s = g & (kTcStages - 1);
-        const uint32_t j = st & (kTcStagesPerBlock - 1), buf = (st / kTcStagesPerBlock) & 1;
-        tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
-        ptx::named_barrier(1, kTcProducers);
-        // B'^T rows: re row `row` = (Re B, Im B), im row NT/2 + row =
-        // (Im B, -Re B), B = e_q(n) W'(n, v).  Pairs past Q_tile VG hold
-        // values no output reads.
-        const float4 *wp = reinterpret_cast<const float4 *>(w_all + (buf * WR + bw) * kWStride + j * kTcNodes + 8 * half);
-        float br[8], bi[8];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float4 w2 = wp[i];
-          br[2 * i] = w2.x; bi[2 * i] = w2.y; br[2 * i + 1] = w2.z; bi[2 * i + 1] = w2.w;
-        }
-        if (fac) {
-          const float4 *ep = reinterpret_cast<const float4 *>(etab + ((st & 1) * Qt + bq) * kEStride + 8 * half);
+      for (uint32_t sg = 0; sg < nst; sg += kTcFacGroup) {
+        const uint32_t s_end = min(nst, sg + (uint32_t)kTcFacGroup);
+        for (uint32_t st = sg; st < s_end; ++st) {
+          const uint32_t g = g0 + st, s = g & (kTcStages - 1);
+          const uint32_t j = st & (kTcStagesPerBlock - 1), buf = (st / kTcStagesPerBlock) & 1;
+          tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
+          // B'^T rows: re row `row` = (Re B, Im B), im row NT/2 + row =
+          // (Im B, -Re B), B = e_q(n) W'(n, v).  Pairs past Q_tile VG hold
+          // values no output reads.
+          const float4 *wp =
+              reinterpret_cast<const float4 *>(w_all + (buf * WR + bw) * kWStride + j * kTcNodes + 8 * half);
+          float br[8], bi[8];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            const float4 e2 = ep[i];
-            const float wr0 = br[2 * i], wi0 = bi[2 * i], wr1 = br[2 * i + 1], wi1 = bi[2 * i + 1];
-            br[2 * i] = e2.x * wr0 - e2.y * wi0;
-            bi[2 * i] = e2.x * wi0 + e2.y * wr0;
-            br[2 * i + 1] = e2.z * wr1 - e2.w * wi1;
-            bi[2 * i + 1] = e2.z * wi1 + e2.w * wr1;
+            const float4 w2 = wp[i];
+            br[2 * i] = w2.x; bi[2 * i] = w2.y; br[2 * i + 1] = w2.z; bi[2 * i + 1] = w2.w;
+          }
+          {
+            const float4 *ep = reinterpret_cast<const float4 *>(etab + ((st & (kTcEBufs - 1)) * Qt + bq) * kEStride +
+                                                                8 * half);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              const float4 e2 = ep[i];
+              const float wr0 = br[2 * i], wi0 = bi[2 * i], wr1 = br[2 * i + 1], wi1 = bi[2 * i + 1];
+              br[2 * i] = e2.x * wr0 - e2.y * wi0;
+              bi[2 * i] = e2.x * wi0 + e2.y * wr0;
+              br[2 * i + 1] = e2.z * wr1 - e2.w * wi1;
+              bi[2 * i + 1] = e2.z * wi1 + e2.w * wr1;
+            }
+          }
+          uint32_t hr[8], lr[8], hm[8], lm[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            split_pair(br[i], bi[i], hr[i], lr[i]);
+            hm[i] = __byte_perm(hr[i], 0u, 0x1032) ^ 0x80000000u;
+            lm[i] = __byte_perm(lr[i], 0u, 0x1032) ^ 0x80000000u;
+          }
+          if (b_rows) {
+            const uint32_t stg = sstages + s * L.stage_bytes;
+            const uint32_t b_st = stg + o_hi;
+            st_shared_v4(b_st, hr[0], hr[1], hr[2], hr[3]);
+            st_shared_v4(b_st + 128, hr[4], hr[5], hr[6], hr[7]);
+            st_shared_v4(b_st + d_lo, lr[0], lr[1], lr[2], lr[3]);
+            st_shared_v4(b_st + d_lo + 128, lr[4], lr[5], lr[6], lr[7]);
+            st_shared_v4(b_st + d_im, hm[0], hm[1], hm[2], hm[3]);
+            st_shared_v4(b_st + d_im + 128, hm[4], hm[5], hm[6], hm[7]);
+            st_shared_v4(b_st + d_im + d_lo, lm[0], lm[1], lm[2], lm[3]);
+            st_shared_v4(b_st + d_im + d_lo + 128, lm[4], lm[5], lm[6], lm[7]);
+          }
+          // the phase table of stage st + kTcFacGroup (next group) into its
+          // buffer, whose last readers (stage st - kTcFacGroup) are past the
+          // previous group's barrier
+          if (t_on0 && st + kTcFacGroup < nst) {
+            const uint32_t st1 = st + kTcFacGroup;
+            const double *pb = pos_all + ((st1 / kTcStagesPerBlock) & 1) * 3 * kTcBlockNodes +
+                               (st1 & (kTcStagesPerBlock - 1)) * kTcNodes;
+            float2 *et = etab + (st1 & (kTcEBufs - 1)) * Qt * kEStride;
+            tc_phase_pair(pb, et, tq, tn, kx0, ky0, kz0);
+            if (t_on1) tc_phase_pair(pb, et, tq + 32, tn, kx1, ky1, kz1);
           }
         }
-        uint32_t hr[8], lr[8], hm[8], lm[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          split_pair(br[i], bi[i], hr[i], lr[i]);
-          hm[i] = __byte_perm(hr[i], 0u, 0x1032) ^ 0x80000000u;
-          lm[i] = __byte_perm(lr[i], 0u, 0x1032) ^ 0x80000000u;
-        }
-        if (b_rows) {
-          const uint32_t stg = sstages + s * L.stage_bytes;
-          const uint32_t b_st = stg + o_hi;
-          st_shared_v4(b_st, hr[0], hr[1], hr[2], hr[3]);
-          st_shared_v4(b_st + 128, hr[4], hr[5], hr[6], hr[7]);
-          st_shared_v4(b_st + d_lo, lr[0], lr[1], lr[2], lr[3]);
-          st_shared_v4(b_st + d_lo + 128, lr[4], lr[5], lr[6], lr[7]);
-          st_shared_v4(b_st + d_im, hm[0], hm[1], hm[2], hm[3]);
-          st_shared_v4(b_st + d_im + 128, hm[4], hm[5], hm[6], hm[7]);
-          st_shared_v4(b_st + d_im + d_lo, lm[0], lm[1], lm[2], lm[3]);
-          st_shared_v4(b_st + d_im + d_lo + 128, lm[4], lm[5], lm[6], lm[7]);
-        }
-        // next stage's phase table into the other parity buffer: its last
-        // readers (stage st - 1) are past this stage's barrier
-        if (t_on0 && st + 1 < nst) {
-          const uint32_t st1 = st + 1;
-          const double *pb = pos_all + ((st1 / kTcStagesPerBlock) & 1) * 3 * kTcBlockNodes +
-                             (st1 & (kTcStagesPerBlock - 1)) * kTcNodes;
-          float2 *et = etab + (st1 & 1) * Qt * kEStride;
-          tc_phase_pair(pb, et, tq, tn, kx0, ky0, kz0);
-          if (t_on1) tc_phase_pair(pb, et, tq + 32, tn, kx1, ky1, kz1);
-        }
         ptx::fence_proxy_async_smem();
-        if ((st & (kTcDrain - 1)) == 0 && st > 0) {
+        ptx::named_barrier(1, kTcProducers);
+        if (s_end < nst && (s_end & (kTcDrain - 1)) == 0) {
           tc_fold(p, B.acc_cols, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
@@ -883,8 +903,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         *kmax = 0;
         *rmax = 0;
       }
-      if (issuer && fac)  // generic groups went out at their own barriers
-        tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, gst - 1, nst - 1, nst);
     }
     if (U.n_groups > 0) tc_final(p, B.acc_cols, W, U, accfull, tmem, gbase + U.n_groups - 1, U.n_groups > 1, abort_flag);
     if (U.n_groups == 0 && tid < U.rows) {
@@ -1205,10 +1223,20 @@ static void carve_batch(Carve &c, const fm_signal_args *probs, int n, TcPlan *pl
 
 // Tile shape of a column group: up to 128 (q, v) pairs per tile and at most
 // 64 kz values (fewer when tuned).
+static void tc_shape(int Qt, int VG, int &NT, int &acc_cols);
+
 static int tc_qt(const fm_signal_args *a, int VG, const fm_tc_tuning *tune) {
   int cap = (128 / VG < 64) ? 128 / VG : 64;
   if (tune && tune->kz_cap > 0 && tune->kz_cap < cap) cap = tune->kz_cap;
-  return (int)((a->n_kz < cap) ? a->n_kz : cap);
+  int Qt = (int)((a->n_kz < cap) ? a->n_kz : cap);
+  // narrower tiles until the tiles, node buffers and phase-table ring fit in
+  // shared memory (stacked runs are limited to what then fits)
+  for (;;) {
+    int NT, acc;
+    tc_shape(Qt, VG, NT, acc);
+    if (Qt <= 8 || tc_smem_layout(NT, VG, Qt).total <= kTcSmemMax) return Qt;
+    Qt -= 8;
+  }
 }
 
 // Runs per stacked unit for a column group: whole slabs only (lines <= 128
@@ -1222,6 +1250,13 @@ static int tc_stack_runs(const fm_signal_args *a, int VG, int Qt) {
   const int by_weights = kTcVGroup / VG;
   if (by_pairs < R) R = by_pairs;
   if (by_weights < R) R = by_weights;
+  // the stacked unit's tiles and weight rows must fit in shared memory
+  while (R > 1) {
+    int NT, acc;
+    tc_shape(Qt, R * VG, NT, acc);
+    if (tc_smem_layout(NT, R * VG, Qt).total <= kTcSmemMax) break;
+    --R;
+  }
   return R < 2 ? 1 : R;
 }
 
