@@ -76,9 +76,18 @@ class BlochSolver:
                        "initial_Mz": initial_Mz if initial_Mz is not None else M0}
         self._host: dict[str, np.ndarray] = {}
         self._dev: dict[str, torch.Tensor] = {}
-        self._dev_nodes = torch.from_numpy(np.ascontiguousarray(self.nodes, dtype=np.float32)).to(self.device)
+        # nodes and every per-node array go up in one transfer; single values are filled
+        pending = [("nodes", np.asarray(self.nodes, np.float32), torch.float32)]
         for name in (*_PARAMS, *_STATE):
-            self._dev[name] = self._snapshot(name)
+            snap = self._snapshot(name)
+            if isinstance(snap, torch.Tensor):
+                self._dev[name] = snap
+            else:
+                pending.append((name, snap, _STATE.get(name, (None, torch.float32))[1]))
+        dev_arrays = ops.upload_many([(a, dt) for _, a, dt in pending], self.device)
+        self._dev_nodes = dev_arrays[0]
+        for (name, _, _), t in zip(pending[1:], dev_arrays[1:]):
+            self._dev[name] = t
 
     @property
     def n_nodes(self) -> int:
@@ -92,10 +101,10 @@ class BlochSolver:
             return (np.asarray(v).reshape(-1, 1) * ones).astype(_STATE[name][0])
         return np.asarray(v, np.float32).reshape(-1, 1) * ones if np.ndim(v) else v * ones
 
-    def _snapshot(self, name: str) -> torch.Tensor:
-        """(N,) device copy of the constructed value: a fill for one value, an
-        upload otherwise (an array of N parameter values is uploaded as given:
-        multiplying it by ones leaves it unchanged)."""
+    def _snapshot(self, name: str):
+        """The constructed value as an (N,) device fill for one value, else as
+        the (N,) host array to upload (an array of N parameter values is taken
+        as given: multiplying it by ones leaves it unchanged)."""
         N = self.n_nodes
         np_t, torch_t = _STATE.get(name, (np.float32, torch.float32))
         v = self._given[name]
@@ -111,7 +120,9 @@ class BlochSolver:
             flat = np.asarray(v, np.float32).reshape(-1)
         else:
             flat = self._construct(name).reshape(-1)
-        return self._upload(flat, np_t)
+        if flat.size != N:
+            raise ValueError(f"BlochSolver: {flat.size} values for {N} nodes")
+        return flat.astype(np_t, copy=False)
 
     def _upload(self, flat: np.ndarray, np_t) -> torch.Tensor:
         if flat.size != self.n_nodes:
@@ -203,9 +214,9 @@ class BlochSolver:
             rfs.append(rf)
             Gs.append(np.ascontiguousarray(G, np.float32).reshape(-1, 3))
             dts.append(np.diff(times, prepend=0).astype(np.float32))
-        up = lambda a, dt=None: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-        ops.bloch_sequence(r0, T1, T2, dB, self.M0, self.gamma, seq, up(np.concatenate(rfs).astype(np.complex64)),
-                           up(np.concatenate(Gs)), up(np.concatenate(dts)), m, z, motion, out_m, out_z,
+        rf, G, dt = ops.upload_many([(np.concatenate(rfs), torch.complex64), (np.concatenate(Gs), torch.float32),
+                                     (np.concatenate(dts), torch.float32)], dev)
+        ops.bloch_sequence(r0, T1, T2, dB, self.M0, self.gamma, seq, rf, G, dt, m, z, motion, out_m, out_z,
                            Mxy_carry=m, Mz_carry=z)
 
     def _solve_blocks(self, blocks, store, r0, T1, T2, dB, m, z, out_m, out_z):
@@ -217,10 +228,9 @@ class BlochSolver:
             if self.pod_trajectory is not None:
                 self.pod_trajectory.update_timeshift(t0)
             dt = np.diff(times, prepend=0).astype(np.float32)
-            inp = ops.BlochInputs(r0=r0, T1=T1, T2=T2, delta_B=dB, M0=self.M0,
-                                  gamma=self.gamma, rf=torch.from_numpy(rf).to(dev),
-                                  G=torch.from_numpy(np.ascontiguousarray(G)).to(dev),
-                                  dt=torch.from_numpy(dt).to(dev), Mxy0=m, Mz0=z)
+            d_rf, d_G, d_dt = ops.upload_many([(rf, torch.complex64), (G, torch.float32), (dt, torch.float32)], dev)
+            inp = ops.BlochInputs(r0=r0, T1=T1, T2=T2, delta_B=dB, M0=self.M0, gamma=self.gamma, rf=d_rf, G=d_G,
+                                  dt=d_dt, Mxy0=m, Mz0=z)
             motion = lower(self.pod_trajectory, N, dev)
             if motion is None:
                 motion = table_motion(sample_table(self.pod_trajectory, bloch_call_times(dt), N, np.float32, dev))

@@ -93,13 +93,11 @@ def _run(rank, M, kloc, t, r0, phi, T2, Mxy, pod, T, precision):
     real = torch.float64 if T == np.float64 else torch.float32
     cplx = torch.complex128 if T == np.float64 else torch.complex64
 
-    def up(a, dtype):
-        return torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dtype)
-
-    inp = ops.SignalInputs(
-        M=ops.SparseCSC(shape, up(indptr, torch.int32), up(indices, torch.int32), up(data, real)),
-        kx=up(kloc[0], real), ky=up(kloc[1], real), kz=up(kloc[2], real), t=up(t, real),
-        r0=up(r0, real), phi=up(phi, real), T2=up(T2, real), Mxy=up(Mxy, cplx))
+    (d_indptr, d_indices, d_data, d_kx, d_ky, d_kz, d_t, d_r0, d_phi, d_T2, d_Mxy) = ops.upload_many(
+        [(indptr, torch.int32), (indices, torch.int32), (data, real), (kloc[0], real), (kloc[1], real),
+         (kloc[2], real), (t, real), (r0, real), (phi, real), (T2, real), (Mxy, cplx)], dev)
+    inp = ops.SignalInputs(M=ops.SparseCSC(shape, d_indptr, d_indices, d_data), kx=d_kx, ky=d_ky, kz=d_kz, t=d_t,
+                           r0=d_r0, phi=d_phi, T2=d_T2, Mxy=d_Mxy)
     motion = lower(pod, N, dev)
     if motion is None:
         calls = signal_call_times(t)

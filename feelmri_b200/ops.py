@@ -53,6 +53,72 @@ def release_workspaces() -> None:
     _ws_cache.clear()
 
 
+_NP_OF = {torch.float32: np.float32, torch.float64: np.float64, torch.int32: np.int32,
+          torch.complex64: np.complex64, torch.complex128: np.complex128}
+_staging: dict = {}
+_staging_lock = None
+_copy_pool = None
+
+
+def upload_many(items, device: torch.device) -> list:
+    """Host arrays -> device tensors in one transfer: each (array, torch dtype)
+    is converted as `torch.from_numpy(a).to(dtype)` would, copied into one
+    pinned staging buffer (on several threads; numpy releases the GIL for
+    large copies) and sent with a single host-to-device copy on the current
+    stream.  The staging buffer is reused once the previous transfer from it
+    has completed (calls from several threads take turns).  Returns the
+    tensors (views of one device allocation)."""
+    global _staging_lock
+    if _staging_lock is None:
+        import threading
+        _staging_lock = threading.Lock()
+    with _staging_lock:
+        return _upload_many(items, device)
+
+
+def _upload_many(items, device: torch.device) -> list:
+    global _copy_pool
+    arrays, offs, total = [], [], 0
+    for a, dt in items:
+        arr = np.ascontiguousarray(np.asarray(a).astype(_NP_OF[dt], copy=False))
+        arrays.append(arr)
+        offs.append(total)
+        total += (arr.nbytes + 255) & ~255
+    key = _index(device)
+    st = _staging.get(key)
+    if st is None or st[0].numel() < total:
+        st = (torch.empty(max(total, 1 << 20), dtype=torch.uint8, pin_memory=True), None)
+    buf, ev = st
+    if ev is not None:
+        ev.synchronize()  # the last transfer out of this buffer is done
+    host = buf.numpy()
+
+    def put(i):
+        arr = arrays[i]
+        if arr.nbytes:
+            np.copyto(host[offs[i]:offs[i] + arr.nbytes].view(arr.dtype).reshape(arr.shape), arr)
+    big = [i for i, arr in enumerate(arrays) if arr.nbytes >= (1 << 20)]
+    for i, arr in enumerate(arrays):
+        if arr.nbytes < (1 << 20):
+            put(i)
+    if len(big) > 1:
+        if _copy_pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+            _copy_pool = ThreadPoolExecutor(max_workers=8)
+        list(_copy_pool.map(put, big))
+    elif big:
+        put(big[0])
+    dev_buf = torch.empty(max(total, 1), dtype=torch.uint8, device=device)
+    dev_buf.copy_(buf[:max(total, 1)], non_blocking=True)
+    ev = torch.cuda.Event()
+    ev.record(torch.cuda.current_stream(device))
+    _staging[key] = (buf, ev)
+    out = []
+    for (a, dt), arr, o in zip(items, arrays, offs):
+        out.append(dev_buf[o:o + arr.nbytes].view(dt).reshape(arr.shape))
+    return out
+
+
 PINNED_RESULT_MAX = 256 << 20
 
 
