@@ -145,8 +145,6 @@ constexpr int kEStride = kTcNodes + 2;
 // (fixed, since the tile layout after them changes from unit to unit).
 constexpr uint32_t kTcFront = 1024;
 constexpr uint32_t kTcBars = 0, kTcMisc = 128;
-// Phase-row slots of a factored unit (int16 source and mirror rows, 128 each).
-constexpr uint32_t kTcSlots = 512;
 
 struct TcSmem {
   uint32_t stage_bytes, a_hi, a_lo, b_hi, b_lo;  // offsets inside a stage
@@ -278,55 +276,6 @@ __device__ inline void tc_note_k(int *kmax, double kx, double ky, double kz) {
 
 __device__ inline void prefetch_l1(const void *ptr) { asm volatile("prefetch.global.L1 [%0];" ::"l"(ptr)); }
 
-// Centring of a factored unit.  The samples of run r of the unit are
-// k(p, q) = kp(r, p) + kq(q) (exact in FP64).  Rows are centred on line
-// m = P_tile / 2 of the tile and kz values on m' = Q_tile / 2, so the phase of
-// sample (p, q) is split into (kp(r, p) - kp(r, m)) + (kq(q) - kq(m')) + kc(r)
-// with kc(r) = kp(r, m) + kq(m') applied per node in the weights.  Centred
-// rows p and 2m - p (kz values q and 2m' - q) whose centred wave vectors are
-// exact negatives (checked in FP64, where differences of float32 values are
-// exact) have conjugate phases: one thread computes the lower one and writes
-// both, which halves the sin/cos work of symmetric Cartesian grids.
-__device__ inline void tc_k3(const TcDev &p, int s, double &x, double &y, double &z) {
-  x = p.kx[s];
-  y = p.ky[s];
-  z = p.kz[s];
-}
-__device__ inline int tc_line_sample(const TcDev &p, const TcUnit &U, int r, int line) {
-  return p.runs[U.it.run + r].start + (U.it.p0 + line) * p.n_kz;
-}
-// kc(r) of run r of a factored unit.
-__device__ inline void tc_center(const TcDev &p, const TcUnit &U, int r, double &x, double &y, double &z) {
-  const int s0 = U.run.start, sq = s0 + U.it.q0 + (U.Q_tile >> 1);
-  double px, py, pz, qx, qy, qz, ox, oy, oz;
-  tc_k3(p, tc_line_sample(p, U, r, U.P_tile >> 1), px, py, pz);
-  tc_k3(p, sq, qx, qy, qz);
-  tc_k3(p, s0, ox, oy, oz);
-  x = px + (qx - ox);
-  y = py + (qy - oy);
-  z = pz + (qz - oz);
-}
-// Centred kz row q of a factored unit's tile and its mirror row (or -1);
-// `source` is false for the upper row of a mirror pair (written by the lower).
-__device__ inline void tc_kz_row(const TcDev &p, const TcUnit &U, int q, double &x, double &y, double &z,
-                                 int &mirror, bool &source) {
-  const int s = U.run.start + U.it.q0, m = U.Q_tile >> 1, pr = 2 * m - q;
-  double mx, my, mz;
-  tc_k3(p, s + q, x, y, z);
-  tc_k3(p, s + m, mx, my, mz);
-  x -= mx;
-  y -= my;
-  z -= mz;
-  bool paired = false;
-  if (pr != q && pr >= 0 && pr < U.Q_tile) {
-    double bx, by, bz;
-    tc_k3(p, s + pr, bx, by, bz);
-    paired = (bx - mx) == -x && (by - my) == -y && (bz - mz) == -z;
-  }
-  source = q <= m || !paired;
-  mirror = (paired && q < m) ? pr : -1;
-}
-
 // Raw node data loaded two stages before it is derived (global loads in
 // flight meanwhile).  With a single rank-1 POD term (the flow and respiratory
 // POD fits of the examples) the node's mode row is loaded into registers with
@@ -418,17 +367,7 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
       const float decay = expf(-tg * (1.0f / r.t2));
       float so, co;
       sincosf(r.phi * tg, &so, &co);
-      float er = decay * co, ei = decay * so;
-      if (U.run.factored) {
-        // the centre's phase factor exp(-2 pi i kc . r) of a factored unit
-        double cx, cy, cz;
-        tc_center(p, U, k, cx, cy, cz);
-        float cc, cs;
-        cycles_cos_sin(fma(cz, (double)z, fma(cy, (double)y, cx * (double)x)), cc, cs);
-        const float fr = er * cc + ei * cs, fi = ei * cc - er * cs;
-        er = fr;
-        ei = fi;
-      }
+      const float er = decay * co, ei = decay * so;
       float2 *wk = wblk + k * p.VG * kWStride;
 #pragma unroll
       for (int v = 0; v < kTcVGroup; ++v)
@@ -493,11 +432,8 @@ __device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, 
 }
 
 // Phase table of one stage of a factored unit: e_q(n) = exp(-2 pi i kq_q . r_n)
-// (kq centred on the tile's middle kz value) for row q and the two nodes n0,
-// n0 + 1 of this thread; row `mirror` (>= 0), whose centred kq is -kq_q,
-// receives the conjugates.
-__device__ inline void tc_phase_pair(const double *pb, float2 *et, int q, int mirror, int n0, double kx, double ky,
-                                     double kz) {
+// for q = q0 (and q0 + 32) and the two nodes n0, n0 + 1 of this thread.
+__device__ inline void tc_phase_pair(const double *pb, float2 *et, int q, int n0, double kx, double ky, double kz) {
   const double2 x = *reinterpret_cast<const double2 *>(pb + n0);
   const double2 y = *reinterpret_cast<const double2 *>(pb + kTcBlockNodes + n0);
   const double2 z = *reinterpret_cast<const double2 *>(pb + 2 * kTcBlockNodes + n0);
@@ -505,7 +441,6 @@ __device__ inline void tc_phase_pair(const double *pb, float2 *et, int q, int mi
   cycles_cos_sin(fma(kz, z.x, fma(ky, y.x, kx * x.x)), c0, s0);
   cycles_cos_sin(fma(kz, z.y, fma(ky, y.y, kx * x.y)), c1, s1);
   *reinterpret_cast<float4 *>(et + q * kEStride + n0) = make_float4(c0, -s0, c1, -s1);
-  if (mirror >= 0) *reinterpret_cast<float4 *>(et + mirror * kEStride + n0) = make_float4(c0, s0, c1, s1);
 }
 
 // Tensor memory: the accumulator in columns [0, NT) and the FP32 running sum
@@ -639,10 +574,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   // applies (cycles_cos_sin)
   int *kmax = reinterpret_cast<int *>(smem + kTcMisc + 8);
   int *rmax = reinterpret_cast<int *>(smem + kTcMisc + 12);
-  // phase-row slots of a factored unit: source row, mirror row (or -1), and
-  // the count of unpaired upper rows
-  int16_t *slot_src = reinterpret_cast<int16_t *>(smem + kTcSlots), *slot_dst = slot_src + kTcRows;
-  int *n_extra = reinterpret_cast<int *>(smem + kTcMisc + 16);
   const uint32_t sbase = ptx::smem_addr(smem);
 
   if (tid == 0) {
@@ -653,7 +584,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     *abort_flag = 0;
     *kmax = 0;
     *rmax = 0;
-    *n_extra = 0;
     ptx::fence_mbar_init();
   }
   if (warp == 0) ptx::tmem_alloc(tmem_slot, 2 * B.acc_cols);
@@ -709,39 +639,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     const uint32_t nst = (uint32_t)U.n_stages;
     ptx::named_barrier(1, kTcProducers);  // the previous unit's readers are done
     // per-unit row data in registers
-    // B: centred kq of phase-table rows tq and tq + 32 and their mirror rows
-    double kx0 = 0, ky0 = 0, kz0 = 0, kx1 = 0, ky1 = 0, kz1 = 0;
+    double kx0 = 0, ky0 = 0, kz0 = 0, kx1 = 0, ky1 = 0, kz1 = 0;  // A: kp of the row; B: kq of q and q + 32
     int bq = 0, bw = 0;  // B: phase-table row and weight row of the pair
-    int e_mir0 = -1, e_mir1 = -1;
-    bool e_src0 = false, e_src1 = false;
     if (a_role) {
-      if (fac && nst > 0 && tid < U.rows) {
-        // Slot of A row tid (row r P_tile + pl of run `run + r`): the lower
-        // rows of mirror pairs and the centre take slots r (m + 1) + pl, the
-        // unpaired upper rows the slots after those.
-        const int r = tid / U.P_tile, pl = tid % U.P_tile, m = U.P_tile >> 1, pr = 2 * m - pl;
-        double ax, ay, az, mx, my, mz;
-        tc_k3(p, tc_line_sample(p, U, r, pl), ax, ay, az);
-        tc_k3(p, tc_line_sample(p, U, r, m), mx, my, mz);
-        bool paired = false;
-        if (pr != pl && pr >= 0 && pr < U.P_tile) {
-          double bx, by, bz;
-          tc_k3(p, tc_line_sample(p, U, r, pr), bx, by, bz);
-          paired = (bx - mx) == -(ax - mx) && (by - my) == -(ay - my) && (bz - mz) == -(az - mz);
-        }
-        int slot = -1;
-        if (pl <= m) slot = r * (m + 1) + pl;
-        else if (!paired) slot = U.it.nrun * (m + 1) + atomicAdd(n_extra, 1);
-        if (slot >= 0) {
-          slot_src[slot] = (int16_t)tid;
-          slot_dst[slot] = (int16_t)((paired && pl < m) ? r * U.P_tile + pr : -1);
-        }
-        if (pl == 0) {
-          // the centre's wave vector joins the phase range check
-          double cx, cy, cz;
-          tc_center(p, U, r, cx, cy, cz);
-          tc_note_k(kmax, cx, cy, cz);
-        }
+      if (row < U.rows) {
+        // row r P_tile + pl belongs to run `run + r` (r = 0 unless stacked)
+        const int r = row / U.P_tile, pl = row % U.P_tile;
+        const int start = r == 0 ? U.run.start : p.runs[U.it.run + r].start;
+        const int s_p = start + (fac ? (U.it.p0 + pl) * p.n_kz : U.it.p0 + pl);
+        kx0 = p.kx[s_p];
+        ky0 = p.ky[s_p];
+        kz0 = p.kz[s_p];
+        if (nst > 0) tc_note_k(kmax, kx0, ky0, kz0);
       }
     } else {
       if (row < U.pairs) {
@@ -750,18 +659,25 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         bq = jv / VG;
         bw = r * VG + jv % VG;
       }
-      if (fac && nst > 0) {
+      if (fac) {
+        const int s_0 = U.run.start;
         if (tq < U.Q_tile) {
-          tc_kz_row(p, U, tq, kx0, ky0, kz0, e_mir0, e_src0);
-          if (e_src0) tc_note_k(kmax, kx0, ky0, kz0);
+          const int s_q = U.run.start + U.it.q0 + tq;
+          kx0 = (double)p.kx[s_q] - (double)p.kx[s_0];
+          ky0 = (double)p.ky[s_q] - (double)p.ky[s_0];
+          kz0 = (double)p.kz[s_q] - (double)p.kz[s_0];
+          if (nst > 0) tc_note_k(kmax, kx0, ky0, kz0);
         }
         if (tq + 32 < U.Q_tile) {
-          tc_kz_row(p, U, tq + 32, kx1, ky1, kz1, e_mir1, e_src1);
-          if (e_src1) tc_note_k(kmax, kx1, ky1, kz1);
+          const int s_q = U.run.start + U.it.q0 + tq + 32;
+          kx1 = (double)p.kx[s_q] - (double)p.kx[s_0];
+          ky1 = (double)p.ky[s_q] - (double)p.ky[s_0];
+          kz1 = (double)p.kz[s_q] - (double)p.kz[s_0];
+          if (nst > 0) tc_note_k(kmax, kx1, ky1, kz1);
         }
       }
     }
-    const bool t_on0 = !a_role && e_src0, t_on1 = !a_role && e_src1;
+    const bool t_on0 = !a_role && fac && tq < U.Q_tile, t_on1 = !a_role && fac && tq + 32 < U.Q_tile;
     const float *wrun = p.weights ? p.weights + (int64_t)U.it.run * p.md.slots : nullptr;
     const uint32_t n_blocks = (nst + kTcStagesPerBlock - 1) / kTcStagesPerBlock;
     // prologue: node block 0 into buffer 0
@@ -774,8 +690,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     // phase tables of the first group's stages (block 0, buffers 0 ..)
     for (uint32_t st = 0; st < kTcFacGroup && st < nst; ++st) {
       float2 *et = etab + st * Qt * kEStride;
-      if (t_on0) tc_phase_pair(pos_all + st * kTcNodes, et, tq, e_mir0, tn, kx0, ky0, kz0);
-      if (t_on1) tc_phase_pair(pos_all + st * kTcNodes, et, tq + 32, e_mir1, tn, kx1, ky1, kz1);
+      if (t_on0) tc_phase_pair(pos_all + st * kTcNodes, et, tq, tn, kx0, ky0, kz0);
+      if (t_on1) tc_phase_pair(pos_all + st * kTcNodes, et, tq + 32, tn, kx1, ky1, kz1);
     }
     const uint32_t g0 = gst;
     int next_drain = 0;
@@ -865,33 +781,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       // j == 4 into the other buffer: that buffer's readers (block blk - 1)
       // are done, and the phase tables of block blk + 1's first stages are
       // computed after the barrier that ends the derive's group.
-      // Each slot's row is written by 4 threads of 4 nodes (up to 64 slots:
-      // warp w takes slots 8 w ..) or by 2 threads of 8 nodes (warp w takes
-      // slots 16 w ..); a thread writes its slot's mirror row too.  Lanes
-      // 8 apart share a slot, so each 8-lane phase of a 16-byte store covers
-      // 8 rows (no bank conflicts), and whole warps past the slots idle (the
-      // issuer's warp 7 among them while at most 56 slots are used).
-      const int S = nst > 0 ? U.it.nrun * ((U.P_tile >> 1) + 1) + *n_extra : 0;
-      const bool quad = S <= 64;
-      const int slot = quad ? rw * 8 + (lane & 7) : rw * 16 + (lane & 15);
-      const int n_off = quad ? 4 * (lane >> 3) : 8 * (lane >> 4), n_chunks = quad ? 1 : 2;
-      const bool active = slot < S;
-      int a_dst = -1;
-      uint32_t o_src = 0, o_dst = 0;
-      double ax = 0, ay = 0, az = 0;  // centred kp of the slot's row
-      if (active) {
-        const int src = slot_src[slot], r = src / U.P_tile, pl = src % U.P_tile;
-        a_dst = slot_dst[slot];
-        double mx, my, mz;
-        tc_k3(p, tc_line_sample(p, U, r, pl), ax, ay, az);
-        tc_k3(p, tc_line_sample(p, U, r, U.P_tile >> 1), mx, my, mz);
-        ax -= mx;
-        ay -= my;
-        az -= mz;
-        tc_note_k(kmax, ax, ay, az);
-        o_src = kmajor_offset(src, 2 * n_off, kTcRows);
-        o_dst = a_dst >= 0 ? kmajor_offset(a_dst, 2 * n_off, kTcRows) : 0;
-      }
+      const bool active = (rw >> 1) * 32 < U.rows;
       for (uint32_t sg = 0; sg < nst; sg += kTcFacGroup) {
         const uint32_t s_end = min(nst, sg + (uint32_t)kTcFacGroup);
         // a group's stages lie in one node block (groups divide the blocks)
@@ -907,34 +797,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           if (st >= s_end) break;
           const uint32_t s = (g0 + st) & (kTcStages - 1), j = jg + i;
           if (active) {
-            // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n;
-            // the mirror row holds (cos, -sin)
-            const uint32_t stg = sstages + s * L.stage_bytes + L.a_hi;
-            const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + n_off;
-#pragma unroll 1
-            for (int c = 0; c < n_chunks; ++c) {
-              uint32_t h[4], l[4];
+            // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n
+            const uint32_t stg = sstages + s * L.stage_bytes;
+            const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 8 * half;
+            uint32_t h[8], l[8];
 #pragma unroll
-              for (int u2 = 0; u2 < 4; u2 += 2) {
-                const double2 x = *reinterpret_cast<const double2 *>(px + 4 * c + u2);
-                const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + 4 * c + u2);
-                const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + 4 * c + u2);
-                float c0, s0, c1, s1;
-                cycles_cos_sin(fma(az, z.x, fma(ay, y.x, ax * x.x)), c0, s0);
-                cycles_cos_sin(fma(az, z.y, fma(ay, y.y, ax * x.y)), c1, s1);
-                split_pair(c0, s0, h[u2], l[u2]);
-                split_pair(c1, s1, h[u2 + 1], l[u2 + 1]);
-              }
-              const uint32_t a_st = stg + o_src + 128 * c;
-              st_shared_v4(a_st, h[0], h[1], h[2], h[3]);
-              st_shared_v4(a_st + d_lo, l[0], l[1], l[2], l[3]);
-              if (a_dst >= 0) {
-                const uint32_t m_st = stg + o_dst + 128 * c;
-                constexpr uint32_t kSin = 0x80000000u;  // sign of the sin half
-                st_shared_v4(m_st, h[0] ^ kSin, h[1] ^ kSin, h[2] ^ kSin, h[3] ^ kSin);
-                st_shared_v4(m_st + d_lo, l[0] ^ kSin, l[1] ^ kSin, l[2] ^ kSin, l[3] ^ kSin);
-              }
+            for (int u4 = 0; u4 < 8; u4 += 2) {
+              const double2 x = *reinterpret_cast<const double2 *>(px + u4);
+              const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
+              const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
+              float c0, s0, c1, s1;
+              cycles_cos_sin(fma(kz0, z.x, fma(ky0, y.x, kx0 * x.x)), c0, s0);
+              cycles_cos_sin(fma(kz0, z.y, fma(ky0, y.y, kx0 * x.y)), c1, s1);
+              split_pair(c0, s0, h[u4], l[u4]);
+              split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
             }
+            const uint32_t a_st = stg + o_hi;
+            st_shared_v4(a_st, h[0], h[1], h[2], h[3]);
+            st_shared_v4(a_st + 128, h[4], h[5], h[6], h[7]);
+            st_shared_v4(a_st + d_lo, l[0], l[1], l[2], l[3]);
+            st_shared_v4(a_st + d_lo + 128, l[4], l[5], l[6], l[7]);
           }
         }
         ptx::fence_proxy_async_smem();
@@ -1007,13 +889,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           // the phase table of stage st + kTcFacGroup (next group) into its
           // buffer, whose last readers (stage st - kTcFacGroup) are past the
           // previous group's barrier
-          if ((t_on0 || t_on1) && st + kTcFacGroup < nst) {
+          if (t_on0 && st + kTcFacGroup < nst) {
             const uint32_t st1 = st + kTcFacGroup;
             const double *pb = pos_all + ((st1 / kTcStagesPerBlock) & 1) * 3 * kTcBlockNodes +
                                (st1 & (kTcStagesPerBlock - 1)) * kTcNodes;
             float2 *et = etab + (st1 & (kTcEBufs - 1)) * Qt * kEStride;
-            if (t_on0) tc_phase_pair(pb, et, tq, e_mir0, tn, kx0, ky0, kz0);
-            if (t_on1) tc_phase_pair(pb, et, tq + 32, e_mir1, tn, kx1, ky1, kz1);
+            tc_phase_pair(pb, et, tq, tn, kx0, ky0, kz0);
+            if (t_on1) tc_phase_pair(pb, et, tq + 32, tn, kx1, ky1, kz1);
           }
         }
         ptx::fence_proxy_async_smem();
@@ -1034,7 +916,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           atomicOr(p.error, kErrPhaseRange);
         *kmax = 0;
         *rmax = 0;
-        *n_extra = 0;
       }
     }
     if (U.n_groups > 0) tc_final(p, B.acc_cols, W, U, accfull, tmem, gbase + U.n_groups - 1, U.n_groups > 1, abort_flag);
