@@ -693,6 +693,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       if (t_on0) tc_phase_pair(pos_all + st * kTcNodes, et, tq, tn, kx0, ky0, kz0);
       if (t_on1) tc_phase_pair(pos_all + st * kTcNodes, et, tq + 32, tn, kx1, ky1, kz1);
     }
+    // the first group's tables are read by other warps than their writers
+    if (fac) ptx::named_barrier(1, kTcProducers);
     const uint32_t g0 = gst;
     int next_drain = 0;
     if (!fac) {
