@@ -106,6 +106,21 @@ def test_deterministic_and_edge_cases(cuda):
                Mxy.astype(np.complex128), None, precision="bf16x3")
 
 
+@pytest.mark.parametrize("res,V", [((4, 140, 6), 17), ((6, 96, 32), 4), ((3, 64, 16), 8)])
+def test_repeat_calls_identical(cuda, res, V):
+    """Several units per block and several column groups: repeated calls give
+    the same bits (the block's warps hand over node blocks, phase tables and
+    stages through barriers only, and the split sums are reduced in a fixed
+    order)."""
+    mesh, N, M, Mxy, phi, T2 = _case(n=1500, V=V)
+    traj = W.cartesian(res=res)
+    r0 = mesh.nodes.astype(np.float32)
+    first = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    for _ in range(3):
+        np.testing.assert_array_equal(Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3"),
+                                      first)
+
+
 def test_deep_node_sums_stay_accurate(cuda):
     """Tens of thousands of nodes per sample: the tensor core's truncating FP32
     accumulation must not grow with the node count (accumulators are drained
