@@ -204,10 +204,12 @@ __device__ inline void split_pair(float a, float b, uint32_t &hi, uint32_t &lo) 
 // 23 bits, sign-extended, are c - rint(c) in units of 2^-23 (error at most
 // 2^-24 cycles, for |c| < 2^28).  This keeps the reduction off the
 // transcendental unit (no rint, no double-to-float conversion): one FP64
-// add, two shifts and an integer-to-float conversion, then the FP32 sin/cos.
+// add, a signed bit-field extract and an integer-to-float conversion, then
+// the FP32 sin/cos.
 __device__ inline void cycles_cos_sin(double c, float &co, float &s) {
   const int lo = __double2loint(__dadd_rn(c, 805306368.0));
-  const int frac = (lo << 9) >> 9;
+  int frac;  // the low 23 bits, sign-extended
+  asm("bfe.s32 %0, %1, 0, 23;" : "=r"(frac) : "r"(lo));
   __sincosf(__int2float_rn(frac) * 7.490140565847157e-07f, &s, &co);  // 2 pi / 2^23
 }
 
