@@ -12,25 +12,28 @@
 //   B = exp(-2 pi i kq . r) W: P = lines rows, Q = kz values times V columns.
 //   Every other run uses P = its samples and Q = 1 (B = W).
 // * Real stacking.  Node n contributes two K entries: A'[p][2n..2n+1] =
-//   (Re A, Im A) and B'^T[(q,v,re)][2n..] = (Re B, -Im B),
-//   B'^T[(q,v,im)][2n..] = (Im B, Re B), so C'[p][2(q,v)+{0,1}] = (Re, Im).
+//   (Re A, -Im A) and, in two blocks of B rows, B'^T[(q,v,re)][2n..] =
+//   (Re B, Im B) and B'^T[(q,v,im)][2n..] = (Im B, -Re B), so column
+//   (q,v,re) of C' is Re C and column (q,v,im) is Im C.
 // * Split BF16.  Each operand x is stored as hi = bf16(x), lo = bf16(x - hi);
 //   hi*hi + hi*lo + lo*hi accumulate in FP32 in tensor memory.
 // * Phases.  k . r is evaluated in FP64 and reduced modulo one cycle (in
 //   fixed point, to 2^-24 cycles) before the FP32 sin/cos, so far nodes at
 //   high k keep their digits.
 //
-// Block (persistent, one per SM): warps 0-7 produce operand tiles (16 nodes
-// per pipeline stage, 4 stages of shared memory in the UMMA no-swizzle
-// K-major layout) and drain the accumulators; one thread of warp 8 issues the
-// MMAs and warp 8 owns the tensor memory.  Stages are handed over with
-// mbarriers; tcgen05.commit frees a stage when the MMAs that read it have
-// completed.  The tensor core's FP32 accumulation truncates, so each
-// accumulator only collects 32 stages: two accumulators alternate in tensor
-// memory and the producers drain the idle one into an FP32 (round-to-nearest)
-// running sum.  Blocks loop over work units (row/column tile of a run x node
-// range).  All waits are bounded: on timeout the block records an error,
-// lets its MMAs finish and frees its tensor memory.
+// Block (persistent, one per SM, 16 warps): in factored units warps 0-7
+// write the A tiles and warps 8-15 the B tiles and the phase tables; in
+// generic units every warp writes A (16 nodes per pipeline stage, a ring of
+// 4 stages in shared memory in the UMMA no-swizzle K-major layout).
+// Threads 0-127 also derive the node blocks.  After each group's
+// barrier one thread (warp 7, lane 0) issues the group's MMAs; warp 0 owns
+// the tensor memory.  tcgen05.commit frees a ring slot when the MMAs that
+// read it have completed.  The tensor core's FP32 accumulation truncates, so
+// the accumulator only collects 32 stages; all warps then fold it into an FP32
+// (round-to-nearest) running sum kept in the other half of tensor memory.
+// Blocks loop over work units (row/column tile of a run x node range).  All
+// waits are bounded: on timeout the block records an error, lets its MMAs
+// finish and frees its tensor memory.
 #include <cmath>
 #include <vector>
 #include <cub/cub.cuh>
