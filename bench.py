@@ -360,6 +360,21 @@ def run_e2e(args, case, w, precision) -> dict:
 
 # -------------------------------------------------------- CPU baseline --
 
+def _host_motion(motion, t: float) -> np.ndarray:
+    """A POD / PODVelocity / PODSum callable evaluated on the host only: the
+    weights as the class computes them (spline at the folded time, times t for
+    velocities, Motion.py:240-290) and the modes x weights product by the
+    oracle's restatement of POD.cpp, so the CPU baseline runs no device code."""
+    import oracle
+    from feelmri_b200.Motion import PODSum, PODVelocity
+    if isinstance(motion, PODSum):
+        return _host_motion(motion.pod1, t) + _host_motion(motion.pod2, t)
+    motion._evaluate_weights(motion._fold_time(t + motion.timeshift))
+    if isinstance(motion, PODVelocity):
+        motion._weights *= t
+    return oracle.tensordot(motion._modes, motion._weights)
+
+
 def cpu_baseline(case, w, budget_s: float = 15.0, threads: int | None = None) -> dict:
     """The C restatement of the reference's Signal (reference compiler flags,
     one thread per core over node ranges, partial k-spaces summed as
@@ -377,7 +392,7 @@ def cpu_baseline(case, w, budget_s: float = 15.0, threads: int | None = None) ->
     while True:
         sl = slice(0, n_ro)
         kx, ky, kz, t = (a[sl] for a in (*traj.points, traj.t))
-        disp = np.stack([case["vel"](float(tt)) for tt in np.unique(t)])
+        disp = np.stack([_host_motion(case["vel"], float(tt)) for tt in np.unique(t)])
         t0 = time.perf_counter()
         oracle.signal(M, kx, ky, kz, t, nodes32, case["phi"], case["T2"], Mxy, disp=disp, dtype=np.float32,
                       threads=threads, flavour="fast")
