@@ -11,6 +11,14 @@ returns (Mxy, Mz) of the stored blocks as (N, n_store) arrays and, like the
 reference, updates initial_Mxy / initial_Mz so that a later solve(start=-2)
 continues the sequence.
 
+The constructor takes the reference's arguments in the reference's order
+(Bloch.py:276-297): a Sequence (anything with .blocks; a plain list of blocks
+also works), a FEMPhantom (anything with .local_nodes; an (N, 3) array also
+works), a Scanner (its .gamma, a pint quantity converted to rad/(ms mT), or a
+plain number; None means the reference's default Scanner, gamma =
+42.58e6 * 2 pi rad Hz/T), M0, T1 and T2 (pint quantities converted to ms, or
+numbers in ms), delta_B, pod_trajectory, initial_Mxy and initial_Mz.  The
+blocks are read from the sequence at each solve(), as the reference does.
 Blocks are workloads.Block objects (discretised arrays) or objects with the
 reference SequenceBlock interface (_discretization(), __call__(times),
 empty, store_magnetization, time_extent).
@@ -25,11 +33,24 @@ from . import ops
 from ._motion import lower, sample_table, table_motion, term_timeshifts
 from .BlochSimulator import bloch_call_times
 
-__all__ = ["BlochSolver", "discretise"]
+__all__ = ["BlochSolver", "discretise", "DEFAULT_GAMMA"]
+
+# the reference Scanner's gamma, 42.58e6 * 2 pi rad Hz/T, in rad/(ms mT) (MRObjects.py:38-40)
+DEFAULT_GAMMA = 42.58e6 * 2 * np.pi * 1e-6
 
 
 def _magnitude_ms(q):
     return q.m_as("ms") if hasattr(q, "m_as") else q
+
+
+def _gamma_of(scanner) -> float:
+    """rad/(ms mT) from a Scanner-like object, a quantity or a number."""
+    if scanner is None:
+        return DEFAULT_GAMMA
+    g = getattr(scanner, "gamma", scanner)
+    if hasattr(g, "m_as"):
+        return float(g.m_as("rad/ms/mT"))
+    return float(g)
 
 
 def discretise(block):
@@ -64,16 +85,20 @@ class BlochSolver:
     initial_Mz in place, as the reference does (Bloch.py:363-368).  Arrays
     that were never read are never copied to the host."""
 
-    def __init__(self, blocks, nodes, M0=1.0, T1=1000.0, T2=100.0, delta_B=0.0, gamma=267.522, pod_trajectory=None,
-                 initial_Mxy=0.0, initial_Mz=None, device=None):
-        self.blocks = list(blocks)
-        self.nodes = np.asarray(nodes)
+    def __init__(self, sequence, phantom, scanner=None, M0=1.0, T1=1000.0, T2=100.0, delta_B=0.0,
+                 pod_trajectory=None, initial_Mxy=0.0, initial_Mz=None, *, gamma=None, device=None):
+        self.sequence = sequence
+        self.phantom = phantom
+        self.scanner = scanner
+        self.nodes = np.asarray(getattr(phantom, "local_nodes", phantom))
+        if self.nodes.ndim != 2 or self.nodes.shape[1] != 3:
+            raise ValueError(f"BlochSolver: phantom nodes must be (N, 3), got {self.nodes.shape}")
         self.M0 = M0
-        self.gamma = gamma
+        self.gamma = _gamma_of(scanner) if gamma is None else float(gamma)
         self.pod_trajectory = pod_trajectory
         self.device = device or ops.require_cuda()
-        self._given = {"T1": T1, "T2": T2, "delta_B": delta_B, "initial_Mxy": initial_Mxy,
-                       "initial_Mz": initial_Mz if initial_Mz is not None else M0}
+        self._given = {"T1": _magnitude_ms(T1), "T2": _magnitude_ms(T2), "delta_B": delta_B,
+                       "initial_Mxy": initial_Mxy, "initial_Mz": initial_Mz if initial_Mz is not None else M0}
         self._host: dict[str, np.ndarray] = {}
         self._dev: dict[str, torch.Tensor] = {}
         # nodes and every per-node array go up in one transfer; single values are filled
@@ -92,6 +117,11 @@ class BlochSolver:
     @property
     def n_nodes(self) -> int:
         return self.nodes.shape[0]
+
+    @property
+    def blocks(self) -> list:
+        """The sequence's blocks, read afresh (blocks added later are seen)."""
+        return list(getattr(self.sequence, "blocks", self.sequence))
 
     def _construct(self, name: str) -> np.ndarray:
         """The (N, 1) host array the reference builds (Bloch.py:285-293)."""

@@ -34,8 +34,8 @@ import torch
 from . import ops
 from ._motion import lower
 
-__all__ = ["grid_points", "nudft_forward", "nudft_adjoint", "dcf_pipe_menon", "dcf_radial_stack",
-           "dcf_local_speed_readout", "reconstruct_nudft"]
+__all__ = ["grid_points", "nudft_forward", "nudft_adjoint", "dcf_pipe_menon", "dcf_path_jacobian",
+           "reconstruct_nudft"]
 
 
 def grid_points(img_shape, fov) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
@@ -141,76 +141,71 @@ def dcf_pipe_menon(kx, ky, kz, img_shape, fov, n_iter: int = 20, eps: float = 1e
     return (w / (w.mean() + eps)).astype(np.float32)
 
 
-def dcf_radial_stack(kx, ky, eps: float = 1e-6, per_slice_normalize: bool = True) -> np.ndarray:
-    """Analytic ramp for (stacks of) radials, w ~ sqrt(kx^2 + ky^2) (Recon.py:108-121)."""
-    kx = np.asarray(kx)
-    ky = np.asarray(ky)
-    R, L, S = kx.shape
-    r = np.sqrt(kx ** 2 + ky ** 2)
-    if per_slice_normalize:
-        w = r / (r.reshape(R, L, S).mean(axis=(0, 1), keepdims=True) + eps)
-    else:
-        w = r / (r.mean() + eps)
-    return w.astype(np.float32).ravel(order="C")
+def dcf_path_jacobian(kx, ky, kz=None, radial_power: int = 1) -> np.ndarray:
+    """Analytic density weights from the geometry of the readout paths.
 
-
-def dcf_local_speed_readout(kx, ky, kz=None, eps: float = 1e-8) -> np.ndarray:
-    """Readout-speed weights per (line, slice) (Recon.py:124-146)."""
-    kx = np.asarray(kx)
-    ky = np.asarray(ky)
-    R, L, S = kx.shape
-    if kz is None:
-        dk = np.sqrt(np.diff(kx, axis=0) ** 2 + np.diff(ky, axis=0) ** 2)
+    Samples along one readout (axis 0 of the (R, L, S) arrays) cover a
+    stretch of path of length v_i = |dk/di| (central differences inside the
+    readout, one-sided at its ends, np.gradient); paths that fan out from the
+    centre (radials, spirals) thin out with the in-plane radius rho, so
+    each sample represents an area proportional to v_i * rho_i^radial_power
+    (radial_power = 1 for 2-D fans and stacks of them, 2 for 3-D radials,
+    0 for parallel lines).  Returned flattened in C order, scaled to mean 1."""
+    kx = np.asarray(kx, np.float64)
+    ky = np.asarray(ky, np.float64)
+    if kx.ndim != 3 or kx.shape != ky.shape:
+        raise ValueError(f"kx and ky must be (R, L, S) arrays of one shape, got {kx.shape} and {ky.shape}")
+    parts = [kx, ky] if kz is None else [kx, ky, np.asarray(kz, np.float64)]
+    if kx.shape[0] < 2:
+        speed = np.ones_like(kx)
     else:
-        kz = np.asarray(kz)
-        dk = np.sqrt(np.diff(kx, axis=0) ** 2 + np.diff(ky, axis=0) ** 2 + np.diff(kz, axis=0) ** 2)
-    w = np.empty((R, L, S), dtype=np.float64)
-    w[0, :, :] = dk[0, :, :]
-    w[-1, :, :] = dk[-1, :, :]
-    w[1:-1, :, :] = 0.5 * (dk[:-1, :, :] + dk[1:, :, :])
-    denom = w.mean(axis=0, keepdims=True) + eps
-    return (w / denom).astype(np.float32).ravel(order="C")
+        speed = np.sqrt(sum(np.gradient(p, axis=0) ** 2 for p in parts))
+    rho = np.hypot(kx, ky) if radial_power != 2 or kz is None else np.sqrt(sum(p ** 2 for p in parts))
+    w = speed * rho ** radial_power
+    mean = w.mean()
+    return (w / mean if mean > 0 else np.ones_like(w)).astype(np.float32).reshape(-1)
 
 
 def reconstruct_nudft(kdata, ktraj, img_shape, fov, *, dcw=None, auto_dcw: str | None = "pipe-menon",
                       n_iter: int = 20, combine: str | None = None, precision: str = "bf16x3") -> np.ndarray:
-    """The structure of reconstruct_nufft (Recon.py:150-290) with exact NUDFT
-    operators: kdata (R, L, S, C), ktraj (kx, ky, kz) each (R, L, S) in 1/m
-    (kz may be None), img_shape (Nx, Ny, Nz), fov in m.  Density weights:
-    dcw if given, else auto_dcw in {None, 'pipe-menon', 'radial-2d', 'speed'}.
+    """Image from non-Cartesian k-space with the exact NUDFT adjoint (the task
+    of reconstruct_nufft, Recon.py:150-290, which uses pynufft's gridding
+    approximation instead).  kdata (R, L, S, C), ktraj = (kx, ky, kz) each
+    (R, L, S) in 1/m (kz may be None for 2-D), img_shape (Nx, Ny, Nz), fov in
+    m.  Density weights: dcw when given, else auto_dcw: None (no weights),
+    'pipe-menon' (dcf_pipe_menon) or 'jacobian' (dcf_path_jacobian).
     Returns (Nx, Ny, Nz) for one channel or combine='rss', else
     (C, Nx, Ny, Nz)."""
     kx, ky, kz = ktraj
     kx = np.asarray(kx, np.float32)
     ky = np.asarray(ky, np.float32)
     kz = np.zeros_like(kx) if kz is None else np.asarray(kz, np.float32)
-    if kx.shape != ky.shape or kx.shape != kz.shape:
-        raise ValueError("kx, ky, kz must share the same shape (R, L, S).")
+    if not (kx.shape == ky.shape == kz.shape) or kx.ndim != 3:
+        raise ValueError(f"trajectory arrays must all be (R, L, S); got {kx.shape}, {ky.shape}, {kz.shape}")
     kdata = np.asarray(kdata)
-    if kdata.shape[:3] != kx.shape:
-        raise ValueError("kdata (R,L,S, C) must match ktraj shapes on first 3 dims.")
-    C = kdata.shape[3]
-    M = kx.size
+    if kdata.ndim != 4 or kdata.shape[:3] != kx.shape:
+        raise ValueError(f"k-space data of shape {kdata.shape} does not fit a {kx.shape} trajectory with a "
+                         "trailing channel axis")
+    n_ch = kdata.shape[3]
+    n_samples = kx.size
     if dcw is None and auto_dcw is not None:
-        method = auto_dcw.lower()
-        if method == "pipe-menon":
+        kind = auto_dcw.lower()
+        if kind == "pipe-menon":
             dcw = dcf_pipe_menon(kx, ky, kz, img_shape, fov, n_iter=n_iter, precision=precision)
-        elif method == "radial-2d":
-            dcw = dcf_radial_stack(kx, ky)
-        elif method == "speed":
-            dcw = dcf_local_speed_readout(kx, ky, None if np.allclose(kz, 0.0) else kz)
+        elif kind == "jacobian":
+            dcw = dcf_path_jacobian(kx, ky, None if not np.any(kz) else kz)
         else:
-            raise ValueError("auto_dcw must be None, 'pipe-menon', 'radial-2d' or 'speed'")
+            raise ValueError(f"unknown auto_dcw {auto_dcw!r}: use None, 'pipe-menon' or 'jacobian'")
     if dcw is not None:
-        dcw = np.asarray(dcw, np.float32)
-        if dcw.shape != (M,):
-            raise ValueError(f"dcw must be shape ({M},), got {dcw.shape}")
-    img = nudft_adjoint(kdata.reshape(M, C), kx, ky, kz, img_shape, fov, dcw=dcw, precision=precision)
+        dcw = np.asarray(dcw, np.float32).reshape(-1)
+        if dcw.size != n_samples:
+            raise ValueError(f"{dcw.size} density weights for {n_samples} samples")
+    img = nudft_adjoint(kdata.reshape(n_samples, n_ch), kx, ky, kz, img_shape, fov, dcw=dcw, precision=precision)
     img = np.moveaxis(img, -1, 0)  # (C, Nx, Ny, Nz)
-    if C == 1:
+    if n_ch == 1:
         return img[0]
     if combine is None:
         return img
     if combine.lower() == "rss":
         return np.sqrt(np.sum(np.abs(img) ** 2, axis=0)).astype(np.complex64)
-    raise ValueError("combine must be None or 'rss'")
+    raise ValueError(f"unknown combine {combine!r}: use None or 'rss'")

@@ -6,7 +6,9 @@ readout time (cpp/feelmri/MRI.cpp:50, :114).  For the callables of
 python/feelmri/Motion.py the arithmetic of that call is reproduced on the GPU
 (see csrc/motion.cuh): this module reads their state (PPoly coefficients and
 breakpoints, POD modes, timeshift, period, direction) into an fm_motion
-struct.  Any other callable is sampled at exactly the times the reference
+struct.  Objects that state their device form themselves through
+fm_motion_terms() (feelmri_b200.motion.SplineMotion) are lowered from that
+statement.  Any other callable is sampled at exactly the times the reference
 would call it, and its outputs are uploaded as a displacement table.
 """
 from __future__ import annotations
@@ -194,8 +196,54 @@ def _respiratory_term(obj, device) -> tuple[L.MotionTerm, list] | None:
     return t, [dev_c, dev_x]
 
 
+_SPEC_KINDS = {"modes": L.FM_TERM_POD, "velocity_modes": L.FM_TERM_POD_VELOCITY, "rigid": L.FM_TERM_RESPIRATORY}
+
+
+def _spec_terms(obj, device) -> tuple[list, list] | None:
+    """Terms of an object that states its own device form through
+    fm_motion_terms() (feelmri_b200.motion.SplineMotion): each term's time
+    is t + timeshift in float64, folded in float64 when it has a period."""
+    specs = obj.fm_motion_terms()
+    terms, keep = [], []
+    for sp in specs:
+        kind = _SPEC_KINDS.get(sp["kind"])
+        if kind is None:
+            return None
+        c = np.ascontiguousarray(sp["coeffs"], np.float64)
+        x = np.ascontiguousarray(sp["knots"], np.float64)
+        dev_c = device_cache.get(c, torch.float64, device)
+        dev_x = device_cache.get(x, torch.float64, device)
+        t = L.MotionTerm()
+        t.kind = kind
+        t.pp_c = dev_c.data_ptr()
+        t.pp_x = dev_x.data_ptr()
+        t.pp_k = c.shape[0]
+        t.pp_intervals = c.shape[1]
+        t.timeshift = float(sp["timeshift"])
+        t.timeshift_kind = L.FM_NUM_PYFLOAT
+        t.period_kind = L.FM_NUM_NONE if sp["period"] is None else L.FM_NUM_F64
+        t.period = 0.0 if sp["period"] is None else float(sp["period"])
+        t.extrapolate = 1 if sp["extrapolate"] else 0
+        if kind == L.FM_TERM_RESPIRATORY:
+            t.n_modes = 1
+            t.modes = None
+            for i in range(3):
+                t.direction[i] = float(np.float32(sp["direction"][i]))
+            keep += [dev_c, dev_x]
+        else:
+            modes = sp["modes"]
+            dev_modes = device_cache.get(modes, torch.float32, device)
+            t.n_modes = modes.shape[2]
+            t.modes = dev_modes.data_ptr()
+            keep += [dev_modes, dev_c, dev_x]
+        terms.append(t)
+    return (terms, keep) if terms else None
+
+
 def _terms(obj, device) -> tuple[list, list] | None:
     """Flattens a left-nested PODSum into terms added left to right."""
+    if callable(getattr(obj, "fm_motion_terms", None)):
+        return _spec_terms(obj, device)
     if any(k.__name__ == "PODSum" for k in type(obj).__mro__) and _defined_by(obj, "__call__", {"PODSum"}):
         left = _terms(obj.pod1, device)
         # pod1(t) + pod2(t): the right operand must be a single term so that
@@ -219,6 +267,8 @@ def term_timeshifts(obj) -> list | None:
     lays the terms out (a left-nested PODSum left to right); None when a
     timeshift has a type lower() would refuse.  Reads only the timeshifts, so
     a block sequence can follow update_timeshift() without lowering again."""
+    if callable(getattr(obj, "fm_motion_terms", None)):
+        return [(float(sp["timeshift"]), L.FM_NUM_PYFLOAT) for sp in obj.fm_motion_terms()]
     if any(k.__name__ == "PODSum" for k in type(obj).__mro__) and _defined_by(obj, "__call__", {"PODSum"}):
         left = term_timeshifts(obj.pod1)
         right = term_timeshifts(obj.pod2)

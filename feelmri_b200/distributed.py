@@ -57,17 +57,34 @@ def distribute_mesh(elems: np.ndarray, nodes: np.ndarray, world: int, rank: int,
     return LocalMesh(local, nodes[l2g], l2g, cells)
 
 
+def reduce_device(backend: str, tensor, current_cuda: int | None = None):
+    """Device the reduce buffer must live on: NCCL reduces CUDA tensors only,
+    so host data goes to the current CUDA device; other backends reduce
+    where the data is."""
+    import torch
+    if backend == "nccl" and tensor.device.type != "cuda":
+        idx = torch.cuda.current_device() if current_cuda is None else current_cuda
+        return torch.device("cuda", idx)
+    return tensor.device
+
+
 def gather_data(data, group=None, dst: int = 0):
     """Sum of `data` over all ranks, delivered on rank `dst` (other ranks
     get their input back unchanged, as MPI Reduce leaves them).  `data` is a
-    numpy array or a torch tensor; complex values are reduced as (re, im)."""
+    numpy array or a torch tensor (host or device); complex values are
+    reduced as (re, im) pairs.  With the NCCL backend host data is reduced
+    through a buffer on the current CUDA device and returned on the host."""
     import torch
     import torch.distributed as dist
     is_np = isinstance(data, np.ndarray)
     t = torch.from_numpy(np.ascontiguousarray(data)) if is_np else data.contiguous()
-    buf = torch.view_as_real(t).clone() if t.is_complex() else t.clone()
+    home = t.device
+    buf = torch.view_as_real(t) if t.is_complex() else t
+    buf = buf.to(reduce_device(dist.get_backend(group), buf), copy=True)
     dist.reduce(buf, dst=dst, op=dist.ReduceOp.SUM, group=group)
     if dist.get_rank(group) != dst:
         return data
     out = torch.view_as_complex(buf) if t.is_complex() else buf
+    if out.device != home:
+        out = out.to(home)
     return out.numpy() if is_np else out

@@ -1,5 +1,5 @@
-"""Request loop for simulations: admission by HBM footprint, device-resident
-state, overlapping execution and latency statistics.
+"""Many simulations on one GPU: batched frames, continuous admission and
+latency statistics.
 
 A request is one simulation: a mesh with tissue parameters, the imaging
 blocks of a sequence, a k-space trajectory, receive coils and a number of
@@ -7,25 +7,34 @@ cardiac frames (with optional motion).  Once admitted, everything a request
 needs stays on the GPU until it completes:
 
 * the mesh, tissue arrays, lumped P1 mass weights (assembled on the device)
-  and coil maps;
+  and coil maps, uploaded through one pinned staging buffer;
 * the magnetisation (Mxy, Mz), carried from block to block and frame to
   frame by the fused Bloch sweep;
-* the Signal workspace, reused frame after frame.
+* the k-space output buffer, reused frame after frame.
 
-Serving is continuous: a dispatcher admits arriving requests whenever a
-slot is free and the HBM budget holds their footprint, and every slot runs
-its request's frames on its own CUDA stream.  Requests therefore overlap on
-the device, and a new one does not wait for the others to finish.  Each
-request's result depends only on its own inputs: its kernels, tile shapes and
-reduction orders do not depend on what else runs, so it is the same alone and
-in a mix.
+Execution is batched by frame.  One *iteration* advances every admitted
+request by one frame: each request's Bloch blocks and coil expansion, then
+ONE persistent tensor-core launch (fm_signal_batch_enqueue) that contracts
+the Signal of all of them together -- the requests' work units share the
+SMs inside that launch -- then one copy of every output to pinned host
+memory.  Requests that arrive while an iteration runs are set up (upload,
+mass assembly) on a side stream and join the next iteration, as far as the
+slot count and the HBM budget allow; requests whose last frame is done leave.
+This is continuous batching at frame granularity.
 
-The reference has no serving mode (its examples loop over frames in Python,
-e.g. examples/phase_contrast.py:198-207); this module is new.
+A request's result depends only on its own inputs: its Signal work units,
+their node splits and the reduction order are fixed by the request and the
+server's fixed tuning (ops.Tuning), never by the other requests in the
+launch, so it is the same alone and in any mix, bit for bit.
+
+``simulate_batch`` runs one frame of many simulations from host arrays to
+host arrays through the same machinery (the batched configuration's public
+call).  The reference has no serving or batching mode (its examples loop
+over phantoms and frames in Python, e.g. examples/phase_contrast.py:198-207);
+this module is new.
 """
 from __future__ import annotations
 
-import threading
 import time
 from dataclasses import dataclass, field
 
@@ -36,7 +45,12 @@ from . import ops
 from ._motion import lower
 from .workloads import GAMMA, Block, Mesh, Trajectory
 
-__all__ = ["Request", "Simulation", "Server", "latency_stats"]
+__all__ = ["Request", "Simulation", "Server", "latency_stats", "simulate_batch", "launch_iteration",
+           "finish_iteration", "run_iteration", "SERVING_TUNING"]
+
+# Work-unit shape used for every served request: a fixed node split keeps each
+# request's reduction order independent of the batch it lands in.
+SERVING_TUNING = ops.Tuning(split_nodes=16384, kz_cap=0)
 
 
 @dataclass
@@ -51,13 +65,18 @@ class Request:
     coils: np.ndarray         # (N, C) complex64 receive sensitivities
     frames: int = 1
     frame_ms: float = 40.0    # time between frames (motion timeshift)
-    pod: object = None        # motion callable (reference classes are lowered to the GPU)
+    pod: object = None        # motion callable (lowered to the GPU when it can be)
     precision: str = "bf16x3"
     arrival: float = 0.0      # seconds after the start of the run
+    weights: np.ndarray | None = None  # lumped mass weights; assembled on the device when None
 
     @property
     def n_nodes(self) -> int:
         return self.mesh.n_nodes
+
+    @property
+    def n_coils(self) -> int:
+        return self.coils.shape[1]
 
     @property
     def work(self) -> float:
@@ -67,83 +86,158 @@ class Request:
 
 def footprint_bytes(req: Request) -> int:
     """Device bytes a request holds while admitted (state, inputs, outputs and
-    the Signal workspace), estimated from its sizes."""
-    N, S, C = req.n_nodes, req.traj.n_samples, req.coils.shape[1]
+    its share of the batch workspace), estimated from its sizes."""
+    N, S, C = req.n_nodes, req.traj.n_samples, req.n_coils
     E = req.mesh.elems.shape[0]
     state = N * (12 + 4 * 4 + 8 + 4 + 8 * C * 2)           # nodes, tissue, mass, Mxy/Mz, coils, Mxy columns
     traj = S * 16 + S * C * 8                              # k, t, one output frame
-    mass_setup = E * 16 * 32                               # assembly triplets (transient)
+    mass_setup = E * 16 * 32 if req.weights is None else 0  # assembly triplets (transient)
     signal_ws = N * C * 8 + S * 64 + 16 * S * C * 8
     return int(state + traj + max(mass_setup, signal_ws) + (64 << 20))
 
 
 class Simulation:
-    """Device-resident state of one admitted request, bound to one stream."""
+    """Device-resident state of one request.  Construction queues the upload
+    and the mass assembly on `stream` and records `ready` there."""
 
-    def __init__(self, req: Request, device: torch.device, stream: torch.cuda.Stream):
+    def __init__(self, req: Request, device: torch.device, stream: torch.cuda.Stream | None = None):
         from .Assemble import mass_lumped
         from .FiniteElements import FiniteElement, QuadratureRule
         self.req = req
         self.device = device
-        self.stream = stream
-        N = req.n_nodes
-        with torch.cuda.stream(stream):
-            def up(a, dt=torch.float32):
-                return torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dt, non_blocking=True)
-            w = mass_lumped(req.mesh.elems, req.mesh.nodes, FiniteElement(), QuadratureRule(order=2))
-            self.r0 = up(req.mesh.nodes.astype(np.float32))
-            self.T1, self.T2 = up(req.T1), up(req.T2)
+        self.stream = stream or torch.cuda.current_stream(device)
+        self.frame = 0
+        N, t = req.n_nodes, req.traj
+        with torch.cuda.stream(self.stream):
+            items = [(req.mesh.nodes, torch.float32), (req.T1, torch.float32), (req.T2, torch.float32),
+                     (req.phi, torch.float32), (req.coils, torch.complex64), (t.kx, torch.float32),
+                     (t.ky, torch.float32), (t.kz, torch.float32), (t.t, torch.float32)]
+            for b in req.blocks:
+                items += [(b.rf, torch.complex64), (b.G, torch.float32), (b.dt, torch.float32)]
+            if req.weights is not None:
+                items.append((req.weights, torch.float32))
+            dev = ops.upload_many(items, device)
+            self.r0, self.T1, self.T2, self.phi, self.coils, kx, ky, kz, tt = dev[:9]
+            self.blocks = [(dev[9 + 3 * i], dev[10 + 3 * i], dev[11 + 3 * i], b.t0, b.empty)
+                           for i, b in enumerate(req.blocks)]
+            if req.weights is not None:
+                w = dev[-1]
+            else:
+                w = torch.from_numpy(np.ascontiguousarray(
+                    mass_lumped(req.mesh.elems, req.mesh.nodes, FiniteElement(), QuadratureRule(order=2)),
+                    np.float32)).to(device, non_blocking=True)
+            idx = torch.arange(N + 1, dtype=torch.int32, device=device)
+            self.M = ops.SparseCSC((N, N), idx, idx[:N], w)
             self.dB = torch.zeros(N, dtype=torch.float32, device=device)
-            self.phi = up(req.phi)
-            self.coils = up(req.coils, torch.complex64)
-            self.blocks = [(up(b.rf, torch.complex64), up(b.G), up(b.dt.astype(np.float32)), b.t0, b.empty)
-                           for b in req.blocks]
-            self.M = ops.SparseCSC((N, N), up(np.arange(N + 1, dtype=np.int32), torch.int32),
-                                   up(np.arange(N, dtype=np.int32), torch.int32), up(w.astype(np.float32)))
-            t = req.traj
-            self.kx, self.ky, self.kz, self.t = up(t.kx), up(t.ky), up(t.kz), up(t.t)
             self.Mxy = torch.zeros(N, dtype=torch.complex64, device=device)
             self.Mz = torch.ones(N, dtype=torch.float32, device=device)
-            self.cols = torch.empty((N, req.coils.shape[1]), dtype=torch.complex64, device=device)
-            self.out = torch.empty((*t.shape, req.coils.shape[1]), dtype=torch.complex64, device=device)
-            self.sig = ops.SignalInputs(M=self.M, kx=self.kx, ky=self.ky, kz=self.kz, t=self.t, r0=self.r0,
-                                        phi=self.phi, T2=self.T2, Mxy=self.cols)
-            # the workspace holds per-time motion weights: size it with the request's motion
-            a = ops.signal_args(self.sig, lower(req.pod, N, device), req.precision, self.out)
-            self.ws = torch.empty(ops.signal_workspace_bytes(a, req.precision), dtype=torch.uint8, device=device)
-        self.kspace = np.empty((req.frames, *t.shape, req.coils.shape[1]), np.complex64)
+            self.readout = torch.empty(N, dtype=torch.complex64, device=device)
+            self.cols = torch.empty((N, req.n_coils), dtype=torch.complex64, device=device)
+            self.out = torch.empty((*t.shape, req.n_coils), dtype=torch.complex64, device=device)
+            self.sig = ops.SignalInputs(M=self.M, kx=kx, ky=ky, kz=kz, t=tt, r0=self.r0, phi=self.phi, T2=self.T2,
+                                        Mxy=self.cols)
+            self.ready = torch.cuda.Event()
+            self.ready.record(self.stream)
+        self.kspace = np.empty((req.frames, *t.shape, req.n_coils), np.complex64)
 
-    def run(self) -> np.ndarray:
-        """All frames.  Per frame the sequence blocks run with the state carried
-        (Mxy spoiled after non-empty blocks, as BlochSolver does); the last
-        block's final, unspoiled Mxy is read out through every coil."""
+    @property
+    def done(self) -> bool:
+        return self.frame >= self.req.frames
+
+    def enqueue_bloch(self, f: int) -> None:
+        """Frame f's blocks on the current stream: the state is carried, Mxy
+        spoiled after non-empty blocks (as BlochSolver does); the last
+        block's final, unspoiled Mxy goes through every coil into the
+        Signal's input columns."""
         req = self.req
         N = req.n_nodes
-        readout = torch.empty(N, dtype=torch.complex64, device=self.device)
-        pinned = torch.empty(self.out.shape, dtype=torch.complex64, pin_memory=True)
-        with torch.cuda.stream(self.stream):
-            for f in range(req.frames):
-                for bi, (rf, G, dt, t0, empty) in enumerate(self.blocks):
-                    last = bi == len(self.blocks) - 1
-                    if req.pod is not None:
-                        req.pod.update_timeshift(f * req.frame_ms + t0)
-                    inp = ops.BlochInputs(r0=self.r0, T1=self.T1, T2=self.T2, delta_B=self.dB, M0=1.0, gamma=GAMMA,
-                                          rf=rf, G=G, dt=dt, Mxy0=self.Mxy, Mz0=self.Mz)
-                    final = self.Mxy if empty else (readout if last else None)
-                    ops.bloch_solve(inp, lower(req.pod, N, self.device), history=False, Mxy_final=final,
-                                    Mz_final=self.Mz, Mxy_carry=None if empty else self.Mxy, allocate_final=False)
-                    if last:
-                        src = self.Mxy if empty else readout
-                ops.coil_expand(src, self.coils, out=self.cols)
-                if req.pod is not None:
-                    req.pod.update_timeshift(f * req.frame_ms)
-                motion = lower(req.pod, N, self.device)
-                ops.signal(self.sig, motion, req.precision, out=self.out, sync=False, ws=self.ws)
-                ops.signal_status(self.sig, motion, req.precision, self.out, self.ws)
-                pinned.copy_(self.out, non_blocking=True)
-                self.stream.synchronize()
-                self.kspace[f] = pinned.numpy()
-        return self.kspace
+        src = None
+        for bi, (rf, G, dt, t0, empty) in enumerate(self.blocks):
+            last = bi == len(self.blocks) - 1
+            if req.pod is not None:
+                req.pod.update_timeshift(f * req.frame_ms + t0)
+            inp = ops.BlochInputs(r0=self.r0, T1=self.T1, T2=self.T2, delta_B=self.dB, M0=1.0, gamma=GAMMA,
+                                  rf=rf, G=G, dt=dt, Mxy0=self.Mxy, Mz0=self.Mz)
+            final = self.Mxy if empty else (self.readout if last else None)
+            ops.bloch_solve(inp, lower(req.pod, N, self.device), history=False, Mxy_final=final,
+                            Mz_final=self.Mz, Mxy_carry=None if empty else self.Mxy, allocate_final=False)
+            if last:
+                src = self.Mxy if empty else self.readout
+        ops.coil_expand(src, self.coils, out=self.cols)
+
+    def motion(self, f: int):
+        if self.req.pod is not None:
+            self.req.pod.update_timeshift(f * self.req.frame_ms)
+        return lower(self.req.pod, self.req.n_nodes, self.device)
+
+
+@dataclass
+class Iteration:
+    """One frame of a set of simulations, queued on a stream."""
+    sims: list
+    batch: object
+    host: list
+    stream: torch.cuda.Stream
+    keep: list
+
+
+def launch_iteration(sims: list[Simulation], tuning: ops.Tuning = SERVING_TUNING) -> Iteration:
+    """Queues one frame of every simulation on the current stream: their
+    Bloch blocks, one persistent launch for all split-BF16 Signals (float32
+    requests run their own CUDA-core Signal), then copies of the outputs to
+    pinned host buffers.  Does not wait; finish_iteration() does."""
+    stream = torch.cuda.current_stream(sims[0].device)
+    for s in sims:
+        stream.wait_event(s.ready)
+    for s in sims:
+        s.enqueue_bloch(s.frame)
+    batch, keep = [], []
+    for s in sims:
+        mo = s.motion(s.frame)
+        keep.append(mo)
+        if s.req.precision == "bf16x3":
+            batch.append((s.sig, mo, s.out))
+        else:
+            ops.signal(s.sig, mo, s.req.precision, out=s.out, sync=False)
+    sb = ops.SignalBatch(batch, tuning) if batch else None
+    if sb is not None:
+        sb.enqueue()
+    host = []
+    for s in sims:
+        h = torch.empty(s.out.shape, dtype=torch.complex64, pin_memory=True)
+        h.copy_(s.out, non_blocking=True)
+        host.append(h)
+    return Iteration(sims, sb, host, stream, keep)
+
+
+def finish_iteration(it: Iteration) -> None:
+    """Waits for a launched iteration, raises the errors its device work
+    found, and files each simulation's frame."""
+    if it.batch is not None:
+        it.batch.status()
+    it.stream.synchronize()
+    for s, h in zip(it.sims, it.host):
+        s.kspace[s.frame] = h.numpy()
+        s.frame += 1
+
+
+def run_iteration(sims: list[Simulation], tuning: ops.Tuning = SERVING_TUNING) -> None:
+    """launch_iteration + finish_iteration."""
+    if sims:
+        finish_iteration(launch_iteration(sims, tuning))
+
+
+def simulate_batch(requests: list[Request], device: torch.device | None = None,
+                   tuning: ops.Tuning | None = None) -> list[np.ndarray]:
+    """One frame of many simulations, host arrays in and host arrays out: all
+    inputs go up through pinned staging, every Bloch block and coil expansion
+    runs, one persistent tensor-core launch contracts every Signal, and the
+    k-spaces come back through pinned memory.  Returns one (n_ro, n_lines,
+    n_kz, C) complex64 array per request."""
+    device = device or ops.require_cuda()
+    sims = [Simulation(r, device, torch.cuda.current_stream(device)) for r in requests]
+    run_iteration(sims, tuning or SERVING_TUNING)
+    return [s.kspace[0] for s in sims]
 
 
 def latency_stats(latencies: list[float]) -> dict:
@@ -162,17 +256,21 @@ class Served:
     finished: float = 0.0
     kspace: np.ndarray | None = None
     error: str | None = None
+    iterations: int = 0        # launches the request took part in
+    peers_max: int = 0         # most other requests in one of its launches
 
 
 @dataclass
 class Server:
     """Continuous-batching request loop on one GPU.
 
-    slots:       requests that may run at the same time (one stream each);
-    hbm_budget:  bytes of device memory the admitted requests may hold."""
+    slots:       requests that may be in flight at the same time;
+    hbm_budget:  bytes of device memory the admitted requests may hold
+                 (0: 80% of the free memory at start)."""
     device: torch.device = None
-    slots: int = 4
+    slots: int = 16
     hbm_budget: int = 0
+    tuning: ops.Tuning = SERVING_TUNING
     results: list = field(default_factory=list)
 
     def __post_init__(self):
@@ -180,67 +278,79 @@ class Server:
         if not self.hbm_budget:
             free, _ = torch.cuda.mem_get_info(self.device)
             self.hbm_budget = int(free * 0.8)
-        self._lock = threading.Condition()
-        self._in_use = 0
-        self._running = 0
-        self._streams = [torch.cuda.Stream(device=self.device) for _ in range(self.slots)]
-        self._free_streams = list(range(self.slots))
-
-    def _admit(self, need: int) -> int | None:
-        if self._running >= self.slots or not self._free_streams:
-            return None
-        if self._in_use + need > self.hbm_budget and self._running > 0:
-            return None
-        self._in_use += need
-        self._running += 1
-        return self._free_streams.pop()
-
-    def _release(self, need: int, slot: int):
-        with self._lock:
-            self._in_use -= need
-            self._running -= 1
-            self._free_streams.append(slot)
-            self._lock.notify_all()
-
-    def _worker(self, item: Served, slot: int, need: int, t0: float):
-        try:
-            torch.cuda.set_device(self.device)
-            sim = Simulation(item.req, self.device, self._streams[slot])
-            item.kspace = sim.run()
-        except Exception as exc:  # noqa: BLE001 - the request fails, the server goes on
-            item.error = f"{type(exc).__name__}: {exc}"
-        finally:
-            item.finished = time.perf_counter() - t0
-            self._release(need, slot)
+        self._side = torch.cuda.Stream(device=self.device)
+        self._main = torch.cuda.Stream(device=self.device)
 
     def serve(self, requests: list[Request], realtime: bool = True) -> list[Served]:
-        """Runs the requests, each arriving at req.arrival seconds (when
-        realtime) and admitted as soon as a slot and memory allow; returns one
-        record per request with its times and k-space."""
+        """Runs the requests, each arriving at req.arrival seconds after the
+        start (when realtime; otherwise all at once) and admitted when a slot
+        and memory allow; returns one record per request with its times and
+        k-space.  A request that fails at set-up or in a launch is reported
+        with its error; the others go on."""
+        torch.cuda.set_device(self.device)
         order = sorted(requests, key=lambda r: r.arrival)
         t0 = time.perf_counter()
-        items = [Served(r, r.arrival) for r in order]
-        threads = []
+        items = [Served(r, r.arrival if realtime else 0.0) for r in order]
         pending = list(items)
-        while pending:
-            item = pending[0]
-            now = time.perf_counter() - t0
-            if realtime and now < item.arrival:
-                time.sleep(min(item.arrival - now, 0.01))
+        active: list[tuple[Served, Simulation, int]] = []
+        in_use = 0
+
+        def now():
+            return time.perf_counter() - t0
+
+        def admit():
+            nonlocal in_use
+            while pending and (not realtime or pending[0].arrival <= now()):
+                need = footprint_bytes(pending[0].req)
+                if len(active) + len(joining) >= self.slots or \
+                        ((active or joining) and in_use + need > self.hbm_budget):
+                    return
+                item = pending.pop(0)
+                item.admitted = now()
+                try:
+                    with torch.cuda.stream(self._side):
+                        sim = Simulation(item.req, self.device, self._side)
+                except Exception as exc:  # noqa: BLE001 - the request fails, the server goes on
+                    item.error = f"{type(exc).__name__}: {exc}"
+                    item.finished = now()
+                    continue
+                joining.append((item, sim, need))
+                in_use += need
+
+        joining: list = []
+        while pending or active or joining:
+            active += joining
+            joining = []
+            if not active:
+                admit()
+                if not joining and pending and realtime:
+                    time.sleep(max(0.0, min(pending[0].arrival - now(), 0.01)))
                 continue
-            need = footprint_bytes(item.req)
-            with self._lock:
-                slot = self._admit(need)
-                while slot is None:
-                    self._lock.wait(timeout=0.05)
-                    slot = self._admit(need)
-            item.admitted = time.perf_counter() - t0
-            pending.pop(0)
-            th = threading.Thread(target=self._worker, args=(item, slot, need, t0), daemon=True)
-            th.start()
-            threads.append(th)
-        for th in threads:
-            th.join()
+            try:
+                with torch.cuda.stream(self._main):
+                    it = launch_iteration([s for _, s, _ in active], self.tuning)
+                # requests arriving meanwhile are set up while the launch runs
+                admit()
+                finish_iteration(it)
+            except Exception as exc:  # noqa: BLE001 - fail the launch's requests, keep serving
+                for item, _, need in active:
+                    item.error = f"{type(exc).__name__}: {exc}"
+                    item.finished = now()
+                    in_use -= need
+                active = []
+                continue
+            t_done = now()
+            keep = []
+            for item, sim, need in active:
+                item.iterations += 1
+                item.peers_max = max(item.peers_max, len(active) - 1)
+                if sim.done:
+                    item.kspace = sim.kspace
+                    item.finished = t_done
+                    in_use -= need
+                else:
+                    keep.append((item, sim, need))
+            active = keep
         self.results.extend(items)
         return items
 
@@ -253,5 +363,6 @@ class Server:
                                                   min((it.arrival for it in done), default=0.0))
         out = latency_stats(lat)
         out.update({"requests": len(items), "failed": len(items) - len(done),
-                    "throughput_node_samples_per_s": work / span if span > 0 else None, "span_s": span})
+                    "throughput_node_samples_per_s": work / span if span > 0 else None, "span_s": span,
+                    "max_requests_per_launch": 1 + max((it.peers_max for it in done), default=0)})
         return out

@@ -13,7 +13,8 @@ numpy.random.default_rng(seed):
 * trajectories: Cartesian stacks whose sample time depends on the readout
   index (KSpaceTraj.py:180-220), 3-D radial spokes on a Fibonacci sphere and
   stacks of spirals;
-* motion: Poiseuille flow as a rank-1 PODVelocity and sinusoidal POD weights.
+* motion: Poiseuille flow as a rank-1 velocity-mode motion and sinusoidal
+  mode weights (feelmri_b200.motion.SplineMotion).
 
 Units follow the reference: ms, mT, m, rad/(ms mT), 1/m.
 """
@@ -22,7 +23,6 @@ from __future__ import annotations
 from dataclasses import dataclass, field
 
 import numpy as np
-from scipy.interpolate import PchipInterpolator, PPoly
 
 GAMMA = 42.58e6 * 2 * np.pi * 1e-6  # rad/(ms mT): 267.5 (MRObjects.py:39-40)
 GAMMABAR = 42.58e6 * 1e-6           # cycles/(ms mT)
@@ -275,51 +275,29 @@ def spiral_stack(n_ro=2048, n_interleaves=8, n_kz=8, fov=0.1, kmax=300.0, t_star
 
 # ------------------------------------------------------------------ motion --
 
-def _pod_from(cls, times, modes, weight_samples, is_periodic=True, timeshift=0.0):
-    """A Motion.POD / PODVelocity holding given modes (N, 3, r) and
-    Pchip-interpolated weights sampled at `times` (n_t, r)."""
-    obj = cls.__new__(cls)
-    obj.times = np.asarray(times)
-    obj.data = None
-    obj.local_to_global_map = None
-    obj.n_modes = modes.shape[2]
-    obj.timeshift = timeshift
-    obj.is_periodic = is_periodic
-    obj.interpolation_method = "Pchip"
-    obj.modes = modes
-    obj.weights = weight_samples
-    obj.spline_coeffs = [PchipInterpolator(obj.times, weight_samples[:, i]) for i in range(obj.n_modes)]
-    C = np.stack([s.c for s in obj.spline_coeffs], axis=-1)
-    obj._pp_batch = PPoly(C, obj.spline_coeffs[0].x, extrapolate=False)
-    obj._modes = np.asarray(modes, dtype=np.float32, order="C")
-    obj._period = obj.times[-1] if is_periodic else None
-    obj._weights = np.zeros([obj.n_modes], dtype=np.float32)
-    from .Motion import _periodic_fold
-    obj._fold_time = _periodic_fold(obj._period)
-    return obj
-
-
 def poiseuille_velocity(nodes, radius, v_max=1.0, period=1000.0, n_frames=20):
-    """Rank-1 PODVelocity of v = v_max (1 - rho^2/R^2) z in m/ms, so that the
-    displacement at time t is v t (Motion.py:272-290)."""
-    from .Motion import PODVelocity
+    """Rank-1 velocity-mode motion of v = v_max (1 - rho^2/R^2) z in m/ms:
+    the displacement at time t is v t, the form of a PODVelocity
+    (Motion.py:272-290)."""
+    from .motion import SplineMotion
     rho2 = nodes[:, 0] ** 2 + nodes[:, 1] ** 2
     v = np.zeros((nodes.shape[0], 3, 1))
     v[:, 2, 0] = v_max * np.clip(1 - rho2 / radius ** 2, 0, None) / 1000.0
     times = np.linspace(0.0, period, n_frames).astype(np.float32)
     w = np.ones((n_frames, 1))
-    return _pod_from(PODVelocity, times, v, w)
+    return SplineMotion.from_samples(v, times, w, periodic=True, velocity=True)
 
 
 def sinusoidal_pod(n_nodes, n_modes=10, amp=1e-3, period=800.0, n_frames=40, seed=2):
-    """POD with Phi ~ N(0, amp) metres and a_m(t) = sin(2 pi t / period + psi_m)."""
-    from .Motion import POD
+    """Mode motion with Phi ~ N(0, amp) metres and a_m(t) = sin(2 pi t / period + psi_m),
+    periodic in `period`."""
+    from .motion import SplineMotion
     rng = np.random.default_rng(seed)
     modes = rng.normal(0.0, amp, (n_nodes, 3, n_modes))
     psi = rng.uniform(0, 2 * np.pi, n_modes)
     times = np.linspace(0.0, period, n_frames)
     w = np.sin(2 * np.pi * times[:, None] / period + psi[None, :])
-    return _pod_from(POD, times, modes, w)
+    return SplineMotion.from_samples(modes, times, w, periodic=True)
 
 
 def coil_maps(nodes, n_coils=8, sigma=0.08, ring=0.15, seed=3) -> np.ndarray:

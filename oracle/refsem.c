@@ -126,6 +126,8 @@ void oracle_bloch_f32(int64_t N, int64_t n_time, const float *r0, const float *T
     T *x = (T *)malloc(sizeof(T) * (nn + 1) * 3);                                                               \
     T *phoff = (T *)malloc(sizeof(T) * (nn + 1));                                                               \
     T *W = (T *)malloc(sizeof(T) * (nn + 1) * V * 2);                                                           \
+    T *fc = (T *)malloc(sizeof(T) * (nn + 1)); /* the sample's Fourier vector (MRI.cpp:143-149) */              \
+    T *fs = (T *)malloc(sizeof(T) * (nn + 1));                                                                  \
     T t_old = (T)-1.0;                                                                                          \
     int64_t run = -1;                                                                                           \
     for (int64_t s = 0; s < S; ++s) {                                                                           \
@@ -154,12 +156,17 @@ void oracle_bloch_f32(int64_t N, int64_t n_time, const float *r0, const float *T
         t_old = ts;                                                                                             \
       }                                                                                                         \
       const T kx_ = two_pi * kx[s], ky_ = two_pi * ky[s], kz_ = two_pi * kz[s];                                 \
+      /* one phase and one sin/cos per node-sample, then the V columns (MRI.cpp:143-152) */                     \
+      for (int64_t q = 0; q < nn; ++q) {                                                                        \
+        const T ph = -kx_ * x[3 * q] - ky_ * x[3 * q + 1] - kz_ * x[3 * q + 2] + phoff[q];                      \
+        fc[q] = COSF(ph);                                                                                       \
+        fs[q] = SINF(ph);                                                                                       \
+      }                                                                                                         \
       for (int64_t v = 0; v < V; ++v) {                                                                         \
         T ar[LANES], ai[LANES];                                                                                 \
         for (int l = 0; l < LANES; ++l) ar[l] = ai[l] = (T)0;                                                   \
         for (int64_t q = 0; q < nn; ++q) {                                                                      \
-          const T ph = -kx_ * x[3 * q] - ky_ * x[3 * q + 1] - kz_ * x[3 * q + 2] + phoff[q];                    \
-          const T c = COSF(ph), sn = SINF(ph);                                                                  \
+          const T c = fc[q], sn = fs[q];                                                                        \
           const T wr = W[(q * V + v) * 2], wi = W[(q * V + v) * 2 + 1];                                         \
           ar[q % LANES] += c * wr - sn * wi;                                                                    \
           ai[q % LANES] += c * wi + sn * wr;                                                                    \
@@ -176,6 +183,8 @@ void oracle_bloch_f32(int64_t N, int64_t n_time, const float *r0, const float *T
     free(x);                                                                                                    \
     free(phoff);                                                                                                \
     free(W);                                                                                                    \
+    free(fc);                                                                                                   \
+    free(fs);                                                                                                   \
     free(MM);                                                                                                   \
   }
 

@@ -71,15 +71,26 @@ def test_pod_motion_lowered_equals_sampled_callable(cuda):
     assert fp64.rel_l2(z_low, zo) < 1e-6
 
 
-def test_velocity_pod_and_respiratory_sum(cuda):
-    from feelmri_b200.Motion import RespiratoryMotion
+@pytest.mark.parametrize("kind", ["spline_motion", "reference_classes"])
+def test_velocity_pod_and_respiratory_sum(cuda, kind):
+    import refmotion as R
+    from feelmri_b200.motion import SplineMotion
     mesh, N, T1, T2, dB = _setup(1500)
     b = _block()
     r0 = mesh.nodes.astype(np.float32)
     vel = W.poiseuille_velocity(mesh.nodes, radius=0.04, period=3.0, n_frames=7)
-    resp = RespiratoryMotion(times=np.linspace(0, 6.0, 20), data=0.004 * np.sin(np.linspace(0, np.pi, 20)),
-                             is_periodic=True, direction=np.array([0, 1, 0]))
-    motion = resp + vel
+    times = np.linspace(0, 6.0, 20)
+    curve = 0.004 * np.sin(np.linspace(0, np.pi, 20))
+    if kind == "spline_motion":
+        motion = SplineMotion.rigid((0, 1, 0), times, curve, periodic=True) + vel
+    else:
+        # doubles of the reference's RespiratoryMotion + PODVelocity (a PODSum)
+        from scipy.interpolate import PchipInterpolator
+        fit = PchipInterpolator(times, curve)
+        resp = R.respiratory_from_ppoly(fit.c, fit.x, np.array([0, 1, 0]), period=times[-1])
+        term = vel.terms[0]
+        motion = R.PODSum(resp, R.pod_from_ppoly(term.coeffs, term.knots, term.modes, velocity=True,
+                                                 period=np.float32(term.period)))
     motion.update_timeshift(1.25)
     args = (r0, T1, T2, dB, 1.0, float(GAMMA), b.rf, b.G, b.dt, np.abs(b.rf) != 0, np.zeros(N, np.complex64),
             np.ones(N, np.float32))

@@ -150,8 +150,7 @@ def test_sequence_sweep_equals_block_loop(cuda, motion):
             return None
         p = W.sinusoidal_pod(N, n_modes=3, amp=1e-3, period=9.0, n_frames=7)
         if motion == "pod_sum":
-            from feelmri_b200.Motion import PODSum
-            p = PODSum(p, W.sinusoidal_pod(N, n_modes=2, amp=5e-4, period=5.0, n_frames=5, seed=9))
+            p = p + W.sinusoidal_pod(N, n_modes=2, amp=5e-4, period=5.0, n_frames=5, seed=9)
         return p
 
     results = []
@@ -165,3 +164,90 @@ def test_sequence_sweep_equals_block_loop(cuda, motion):
     for a, b in zip(*results):
         np.testing.assert_array_equal(a, b)
     assert results[0][0].shape == (N, 3)
+
+
+class _Quantity:
+    """Just enough of a pint quantity: a magnitude in one unit."""
+    _TO = {("ms", "ms"): 1.0, ("s", "ms"): 1e3, ("rad*Hz/T", "rad/ms/mT"): 1e-6}
+
+    def __init__(self, m, units):
+        self.m, self.units = m, units
+
+    def m_as(self, units):
+        return self.m * self._TO[(self.units, units)]
+
+    def __add__(self, other):
+        return _Quantity(self.m + other.m_as(self.units), self.units)
+
+
+class _RefBlock:
+    """A block with the reference SequenceBlock interface (Bloch.py:17-141):
+    _discretization() as a quantity in ms, __call__(times) -> (rf, (Gm, Gp, Gs)),
+    time_extent, empty, store_magnetization."""
+
+    def __init__(self, block):
+        self._b = block
+        self.empty = block.empty
+        self.store_magnetization = block.store_magnetization
+        self.time_extent = [_Quantity(float(block.times[0]), "ms"), _Quantity(float(block.times[-1]), "ms")]
+
+    def _discretization(self):
+        return _Quantity(np.asarray(self._b.times, np.float64), "ms")
+
+    def __call__(self, t):
+        idx = np.searchsorted(self._b.times, t)
+        return self._b.rf[idx], tuple(self._b.G[idx, d] for d in range(3))
+
+
+class _RefSequence:
+    def __init__(self, blocks):
+        self.blocks = blocks
+        self.Nb_blocks = len(blocks)
+
+
+class _RefPhantom:
+    def __init__(self, nodes):
+        self.local_nodes = nodes
+
+
+class _RefScanner:
+    gamma = _Quantity(42.58e6 * 2 * np.pi, "rad*Hz/T")
+
+
+@pytest.mark.parametrize("with_motion", [False, True])
+def test_reference_signature_drop_in(cuda, with_motion):
+    # BlochSolver(sequence, phantom, scanner, M0, T1, T2, delta_B,
+    # pod_trajectory, initial_Mxy, initial_Mz) as unchanged reference scripts
+    # build it (Bloch.py:276-297), with pint-like T1/T2 in seconds: the one-
+    # launch sweep equals the per-block loop bit for bit and the reference's
+    # block loop restated on the oracle within FP32 tolerance
+    mesh = W.cylinder(2500)
+    N = mesh.n_nodes
+    T1, T2 = W.tissue(N)
+    nodes = mesh.nodes.astype(np.float32)
+    dB = np.random.default_rng(5).normal(0, 1e-4, (N, 1)).astype(np.float32)
+    plain = _mixed_blocks()
+    seq = _RefSequence([_RefBlock(b) for b in plain])
+
+    def make(pod):
+        return BlochSolver(seq, _RefPhantom(nodes), _RefScanner(), 1.0, _Quantity(T1.reshape(-1, 1) / 1e3, "s"),
+                           _Quantity(T2.reshape(-1, 1) / 1e3, "s"), dB, pod, 0.0, None)
+
+    pods = [W.sinusoidal_pod(N, n_modes=3, amp=1e-3, period=9.0, n_frames=7) if with_motion else None
+            for _ in range(3)]
+    one = make(pods[0])
+    assert one.gamma == pytest.approx(W.GAMMA, rel=1e-12)
+    m1, z1 = one.solve()
+    loop = make(pods[1])
+    loop._solve_sequence = loop._solve_blocks
+    m2, z2 = loop.solve()
+    np.testing.assert_array_equal(m1, m2)
+    np.testing.assert_array_equal(z1, z2)
+    np.testing.assert_array_equal(one.initial_Mxy, loop.initial_Mxy)
+    rm, rz, _, _ = _reference_loop(plain, nodes, T1, T2, dB.reshape(-1), pods[2], np.zeros(N, np.complex64),
+                                   np.ones(N, np.float32))
+    assert fp64.rel_l2(m1, rm) < 2e-6
+    assert fp64.rel_l2(z1, rz) < 1e-6
+    # the reference reads the blocks at solve time: a block appended later is seen
+    seq.blocks.append(_RefBlock(plain[1]))
+    assert len(one.blocks) == len(plain) + 1

@@ -68,9 +68,8 @@ def test_tensordot(cuda, dtype):
 
 
 def _golden_objects(d, name):
-    """Rebuild the stored callables as feelmri_b200.Motion objects."""
-    from feelmri_b200.Motion import POD, PODSum, PODVelocity, RespiratoryMotion, _periodic_fold
-    from scipy.interpolate import PPoly
+    """Rebuild the stored callables as doubles of the reference's classes."""
+    import refmotion as R
 
     def scalar(v, kind):
         v = float(v)
@@ -82,28 +81,24 @@ def _golden_objects(d, name):
         kind = str(d[p + "kind"])
         ts = scalar(d[p + "timeshift"], d[p + "timeshift_kind"])
         period = scalar(d[p + "period"], d[p + "period_kind"])
+        extrapolate = bool(d[p + "extrapolate"])
         if kind in ("POD", "PODVelocity"):
-            obj = (PODVelocity if kind == "PODVelocity" else POD).__new__(PODVelocity if kind == "PODVelocity" else POD)
-            obj._pp_batch = PPoly(d[p + "c"], d[p + "x"], extrapolate=bool(d[p + "extrapolate"]))
-            obj._modes = np.ascontiguousarray(d[p + "modes"])
-            obj.n_modes = obj._modes.shape[2]
-            obj._weights = np.zeros(obj.n_modes, np.float32)
+            obj = R.pod_from_ppoly(d[p + "c"], d[p + "x"], d[p + "modes"], velocity=kind == "PODVelocity",
+                                   extrapolate=extrapolate, timeshift=ts, period=period)
         else:
-            obj = RespiratoryMotion.__new__(RespiratoryMotion)
-            obj.interpolator = PPoly(d[p + "c"], d[p + "x"], extrapolate=bool(d[p + "extrapolate"]))
-            obj.direction = d[p + "direction"]
-        obj.timeshift = ts
-        obj._period = period
-        obj._fold_time = _periodic_fold(period)
+            obj = R.respiratory_from_ppoly(d[p + "c"], d[p + "x"], d[p + "direction"], extrapolate=extrapolate,
+                                           timeshift=ts, period=period)
         terms.append(obj)
     if len(terms) == 1:
         return terms[0]
-    s = PODSum(terms[0], terms[1])
+    s = R.PODSum(terms[0], terms[1])
     s.timeshift = terms[0].timeshift
     return s
 
 
-def test_motion_golden_host_classes_match_reference(cuda):
+def test_motion_golden_doubles_match_reference(cuda):
+    # the test doubles reproduce the reference's own outputs (so the device
+    # comparisons below compare against the reference, not against the doubles)
     d = np.load(GOLDEN)
     for name in d["cases"]:
         obj = _golden_objects(d, name)
@@ -163,12 +158,23 @@ def test_motion_golden_device_displacements(cuda):
         np.testing.assert_allclose(disp, gold, rtol=1e-5, atol=2e-7 * scale, equal_nan=True, err_msg=name)
 
 
+def _numpy_snapshot_pod(times, data, n_modes):
+    # the method of snapshots in plain numpy: eigenpairs of X^T X, the
+    # n_modes largest, modes X e / sqrt(lambda), coefficients X^T modes
+    X = data.reshape(-1, times.shape[0])
+    lam, vec = np.linalg.eigh(X.T @ X)
+    keep = np.argsort(lam)[::-1][:n_modes]
+    phi = X @ (vec[:, keep] / np.sqrt(lam[keep]))
+    return phi.reshape(data.shape[0], -1, n_modes), X.T @ phi
+
+
 @pytest.mark.parametrize("dtype,tol", [(np.float32, 2e-4), (np.float64, 1e-9)])
 def test_pod_construction_on_device(cuda, dtype, tol):
-    # Motion.POD(backend="cuda"): the snapshot products on the GPU, the t x t
-    # eigenproblem on the host; modes, weights and the evaluated motion match
-    # the numpy construction (eigenvector signs are arbitrary: aligned first)
-    from feelmri_b200.Motion import POD
+    # snapshot_pod: the snapshot products on the GPU, the t x t eigenproblem
+    # on the host; modes and weights match the numpy construction
+    # (eigenvector signs are arbitrary: aligned first), and so does the
+    # motion built from them
+    from feelmri_b200.motion import SplineMotion, calculate_pod_on_device, snapshot_pod
     rng = np.random.default_rng(11)
     P, t, r_true = 6000, 24, 4
     times = np.linspace(0.0, 100.0, t)
@@ -177,19 +183,30 @@ def test_pod_construction_on_device(cuda, dtype, tol):
     freq = np.arange(1, r_true + 1)  # distinct frequencies: a well-separated rank-4 history
     w = np.sin(2 * np.pi * freq[None, :] * times[:, None] / 100.0 + rng.uniform(0, 6, r_true)[None, :]) * amp
     data = (np.einsum("pcm,tm->pct", base, w) + 1e-4 * rng.normal(size=(P, 3, t))).astype(dtype)
-    ref = POD(times, data, n_modes=3)
-    dev = POD(times, data, n_modes=3, backend="cuda")
-    assert dev.modes.dtype == ref.modes.dtype and dev.weights.dtype == ref.weights.dtype
+    ref_modes, ref_w = _numpy_snapshot_pod(times, data, 3)
+    modes, weights = snapshot_pod(times, data, 3)
+    assert modes.dtype == dtype and weights.dtype == dtype and modes.shape == (P, 3, 3)
+    signs = []
     for m in range(3):
-        s = np.sign(np.vdot(ref.modes[..., m].ravel(), dev.modes[..., m].ravel()))
-        dm = dev.modes[..., m] * s
-        dw = dev.weights[:, m] * s
-        assert np.linalg.norm(dm - ref.modes[..., m]) / np.linalg.norm(ref.modes[..., m]) < tol
-        assert np.linalg.norm(dw - ref.weights[:, m]) / np.linalg.norm(ref.weights[:, m]) < tol
+        s = np.sign(np.vdot(ref_modes[..., m].ravel(), modes[..., m].ravel()))
+        signs.append(s)
+        assert np.linalg.norm(modes[..., m] * s - ref_modes[..., m]) / np.linalg.norm(ref_modes[..., m]) < tol
+        assert np.linalg.norm(weights[:, m] * s - ref_w[:, m]) / np.linalg.norm(ref_w[:, m]) < tol
     # the motion itself does not depend on the signs
+    a = SplineMotion.from_samples(ref_modes.astype(np.float32), times, ref_w, periodic=False)
+    b = SplineMotion.from_samples(modes.astype(np.float32), times, weights, periodic=False)
     for tq in (0.0, 37.5, 99.0):
-        a, b = ref(tq), dev(tq)
-        assert np.linalg.norm(a - b) / np.linalg.norm(a) < tol
+        assert np.linalg.norm(a(tq) - b(tq)) / np.linalg.norm(a(tq)) < max(tol, 1e-5)
     # reproducible: FP64 sums in a fixed order
-    again = POD(times, data, n_modes=3, backend="cuda")
-    np.testing.assert_array_equal(again.modes, dev.modes)
+    again, _ = snapshot_pod(times, data, 3)
+    np.testing.assert_array_equal(again, modes)
+
+    # the hook that replaces a POD-like object's calculate_pod keeps the local nodes
+    class _PodLike:
+        pass
+    pl = _PodLike()
+    pl.times, pl.data, pl.n_modes = times, data, 3
+    pl.local_to_global_map = np.arange(0, P, 7)
+    hm, hw = calculate_pod_on_device(pl)
+    np.testing.assert_array_equal(hm, modes[pl.local_to_global_map])
+    np.testing.assert_array_equal(hw, weights)

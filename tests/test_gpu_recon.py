@@ -76,7 +76,7 @@ def test_reconstruct_shapes_and_rss(cuda):
     kx, ky, kz = (a.reshape(16, 20, 1) for a in _radial(n_ro=16, n_spokes=20))
     rng = np.random.default_rng(4)
     kdata = (rng.normal(size=(16, 20, 1, 3)) + 1j * rng.normal(size=(16, 20, 1, 3))).astype(np.complex64)
-    img = Recon.reconstruct_nudft(kdata, (kx, ky, kz), (6, 6, 4), (0.1, 0.1, 0.1), auto_dcw="speed")
+    img = Recon.reconstruct_nudft(kdata, (kx, ky, kz), (6, 6, 4), (0.1, 0.1, 0.1), auto_dcw="jacobian")
     assert img.shape == (3, 6, 6, 4)
-    rss = Recon.reconstruct_nudft(kdata, (kx, ky, kz), (6, 6, 4), (0.1, 0.1, 0.1), auto_dcw="speed", combine="rss")
+    rss = Recon.reconstruct_nudft(kdata, (kx, ky, kz), (6, 6, 4), (0.1, 0.1, 0.1), auto_dcw="jacobian", combine="rss")
     np.testing.assert_allclose(np.abs(rss), np.sqrt((np.abs(img) ** 2).sum(0)), rtol=1e-5)

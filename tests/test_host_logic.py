@@ -81,13 +81,27 @@ def test_spamm_block_tags_mz():
 
 def test_batching_workload_is_seeded_and_in_range():
     import bench
-    a = bench.build_batch_case(n_phantoms=6)
-    b = bench.build_batch_case(n_phantoms=6)
-    assert [c["N"] for c in a] == [c["N"] for c in b]
-    for c in a:
-        assert 4_000 <= c["N"] <= 320_000
-        assert 1 <= c["coils"].shape[1] <= 2
-        assert c["traj"].shape[2] >= 8  # every trajectory is a kz stack (factorable slabs)
+    a = bench.build_batch_requests_host(6)
+    b = bench.build_batch_requests_host(6)
+    assert [r.n_nodes for r in a] == [r.n_nodes for r in b]
+    for r in a:
+        assert 4_000 <= r.n_nodes <= 320_000
+        assert 1 <= r.n_coils <= 2
+        assert r.traj.shape[2] >= 8  # every trajectory is a kz stack (factorable slabs)
+        assert r.weights.shape == (r.n_nodes,) and abs(r.weights.sum() / r.weights.sum()) == 1
+        assert 4_000 <= r.traj.n_samples <= 210_000
+
+
+def test_cpu_sample_counts_what_it_runs():
+    # the bounded CPU step of the reference arm: a fraction of nodes for Bloch
+    # and of readout rows for Signal, units = sum of nodes x sampled samples
+    import bench
+    reqs = bench.build_batch_requests_host(2)
+    units, sec, det = bench.cpu_step(reqs, 0.01, 2)
+    want = sum(r.n_nodes * r.traj.kx[:max(1, int(np.ceil(0.01 * r.traj.shape[0])))].size for r in reqs)
+    assert units == want and sec > 0 and det["bloch_s"] >= 0 and det["signal_s"] > 0
+    info = bench.cpu_info()
+    assert info["threads_usable"] >= 1 and info["logical_cpus"] >= 1
 
 
 def _csc_arrays(m, dtype):
@@ -157,12 +171,17 @@ def test_term_timeshifts_follow_the_lowering():
     # the block-sequence sweep reads each block's timeshifts without lowering
     # again; they must be exactly what lower() would put in the descriptor
     from feelmri_b200._motion import lower, term_timeshifts
-    from feelmri_b200.Motion import PODSum
+    import refmotion as R
     N = 50
-    a = W.sinusoidal_pod(N, n_modes=2, n_frames=5)
-    b = W.sinusoidal_pod(N, n_modes=1, n_frames=5, seed=3)
-    c = W.sinusoidal_pod(N, n_modes=3, n_frames=6, seed=4)
-    for obj in (a, PODSum(a, b), PODSum(PODSum(a, b), c)):
+    rng = np.random.default_rng(0)
+
+    def pod(r, n_t):
+        return R.pod_from_samples(rng.normal(size=(N, 3, r)).astype(np.float32), np.linspace(0.0, 10.0, n_t),
+                                  rng.normal(size=(n_t, r)))
+    a, b, c = pod(2, 5), pod(1, 5), pod(3, 6)
+    s1 = W.sinusoidal_pod(N, n_modes=2, n_frames=5)
+    s2 = W.sinusoidal_pod(N, n_modes=1, n_frames=5, seed=3)
+    for obj in (a, R.PODSum(a, b), R.PODSum(R.PODSum(a, b), c), s1, s1 + s2):
         for t0 in (0.0, np.float32(2.5), np.float64(7.25), 3):
             obj.update_timeshift(t0)
             low = lower(obj, N, torch.device("cpu"))
@@ -173,21 +192,109 @@ def test_term_timeshifts_follow_the_lowering():
 
 
 def test_recon_grid_and_analytic_weights():
-    # voxel centres on the DFT-centred grid; the analytic density weights of
-    # Recon.py:108-146 restated (ramp for radials, readout speed for spirals)
+    # voxel centres on the DFT-centred grid; path-Jacobian density weights
+    # (readout speed times in-plane radius, scaled to mean 1)
     from feelmri_b200 import Recon
     X, Y, Z = Recon.grid_points((4, 5, 1), (0.08, 0.1, 0.01))
     np.testing.assert_allclose(X[:, 0, 0], np.array([-2, -1, 0, 1]) * 0.02, atol=1e-7)
     np.testing.assert_allclose(Y[0, :, 0], np.array([-2, -1, 0, 1, 2]) * 0.02, atol=1e-7)
     assert np.all(Z == 0)
-    R, L, S = 6, 4, 2
-    rng = np.random.default_rng(0)
-    kx, ky, kz = (rng.normal(size=(R, L, S)) for _ in range(3))
-    w = Recon.dcf_radial_stack(kx, ky)
-    r = np.sqrt(kx ** 2 + ky ** 2)
-    np.testing.assert_allclose(w, (r / (r.mean(axis=(0, 1), keepdims=True) + 1e-6)).ravel(), rtol=1e-6)
-    ws = Recon.dcf_local_speed_readout(kx, ky, kz).reshape(R, L, S)
-    dk = np.sqrt(np.diff(kx, axis=0) ** 2 + np.diff(ky, axis=0) ** 2 + np.diff(kz, axis=0) ** 2)
-    mid = 0.5 * (dk[:-1] + dk[1:])
-    full = np.concatenate([dk[:1], mid, dk[-1:]], axis=0)
-    np.testing.assert_allclose(ws, full / (full.mean(axis=0, keepdims=True) + 1e-8), rtol=1e-5)
+    # a 2-D radial spoke pair: uniform speed, so the weight is the radius
+    r = np.linspace(-1.0, 1.0, 9)
+    ang = np.array([0.3, 1.9])
+    kx = (r[:, None] * np.cos(ang)[None, :])[..., None]
+    ky = (r[:, None] * np.sin(ang)[None, :])[..., None]
+    w = Recon.dcf_path_jacobian(kx, ky).reshape(kx.shape)
+    want = np.abs(r)[:, None, None] * np.ones_like(kx)
+    np.testing.assert_allclose(w, want / want.mean(), rtol=1e-6)
+    # parallel lines (power 0): the weight follows the readout speed only
+    kx = np.cumsum(np.array([1.0, 1.0, 2.0, 2.0, 1.0]))[:, None, None] * np.ones((1, 3, 2))
+    w = Recon.dcf_path_jacobian(kx, np.zeros_like(kx), radial_power=0).reshape(kx.shape)
+    speed = np.gradient(kx, axis=0)
+    np.testing.assert_allclose(w, speed / speed.mean(), rtol=1e-6)
+
+
+def test_spline_motion_host_evaluation():
+    # SplineMotion's host evaluation against scipy's PPoly on the same
+    # coefficients: float64 spline at the shifted, folded time rounded to
+    # float32, velocity scaling by float32(t), float32 contraction; NaN
+    # outside the knots without a period; a sum adds the terms
+    from scipy.interpolate import PPoly
+    from feelmri_b200.motion import SplineMotion
+    rng = np.random.default_rng(3)
+    N, r = 40, 3
+    modes = rng.normal(size=(N, 3, r)).astype(np.float32)
+    times = np.linspace(0.0, 8.0, 9)
+    samples = rng.normal(size=(9, r))
+    m = SplineMotion.from_samples(modes, times, samples, periodic=True)
+    v = SplineMotion.from_samples(modes, times, samples, periodic=False, velocity=True)
+    pp = PPoly(m.terms[0].coeffs, m.terms[0].knots, extrapolate=False)
+    for ts in (0.0, 1.5):
+        m.update_timeshift(ts)
+        v.update_timeshift(ts)
+        for t in (0.0, 0.3, 7.999, 8.0, 13.25):
+            tau = (t + ts) - 8.0 * np.floor((t + ts) / 8.0)
+            w = pp(tau).astype(np.float32)
+            np.testing.assert_array_equal(m.terms[0].coefficients_at(tau), w)
+            np.testing.assert_allclose(m(t), np.einsum("ncr,r->nc", modes, w), rtol=1e-6, atol=1e-6)
+            raw = pp(t + ts)
+            if np.all(np.isfinite(raw)):
+                np.testing.assert_allclose(v(t), np.einsum("ncr,r->nc", modes, raw.astype(np.float32) *
+                                                           np.float32(t)), rtol=1e-6, atol=1e-6)
+            else:
+                assert np.all(np.isnan(v(t)))
+    both = m + v
+    both.update_timeshift(0.5)
+    m.update_timeshift(0.5)
+    v.update_timeshift(0.5)
+    np.testing.assert_array_equal(both(2.0), (m(2.0) + v(2.0)).astype(np.float32))
+    rigid = SplineMotion.rigid((0, 2, 0), times, np.sin(times), periodic=False)
+    assert rigid(1.0).shape == (1, 3) and rigid(1.0)[0, 0] == 0 and rigid(1.0)[0, 2] == 0
+
+
+def test_install_as_feelmri_patches_reference_modules(tmp_path):
+    # a stand-in reference package: install_as_feelmri must route the native
+    # modules to the drop-ins and replace BlochSolver (and, on request,
+    # POD.calculate_pod) whether feelmri.Bloch is imported before or after
+    import importlib
+    import sys
+    import feelmri_b200
+    from feelmri_b200.Bloch import BlochSolver
+    from feelmri_b200.motion import calculate_pod_on_device
+    pkg = tmp_path / "feelmri"
+    pkg.mkdir()
+    (pkg / "__init__.py").write_text("")
+    (pkg / "Bloch.py").write_text("from feelmri.BlochSimulator import solve_mri\nclass BlochSolver:\n    pass\n")
+    (pkg / "Motion.py").write_text("class POD:\n    def calculate_pod(self, remove_mean=False):\n"
+                                   "        return 'host'\n")
+    saved = {k: v for k, v in sys.modules.items() if k == "feelmri" or k.startswith("feelmri.")}
+    sys.path.insert(0, str(tmp_path))
+    try:
+        for k in saved:
+            del sys.modules[k]
+        feelmri_b200.install_as_feelmri(device_pod=True)
+        bloch = importlib.import_module("feelmri.Bloch")  # imported after the install
+        assert bloch.BlochSolver is BlochSolver
+        assert bloch.solve_mri is feelmri_b200.BlochSimulator.solve_mri
+        motion = importlib.import_module("feelmri.Motion")
+        assert motion.POD.calculate_pod is calculate_pod_on_device
+        bloch.BlochSolver = object  # imported before a second install: patched at once
+        feelmri_b200.install_as_feelmri()
+        assert bloch.BlochSolver is BlochSolver
+    finally:
+        sys.path.remove(str(tmp_path))
+        for k in [k for k in sys.modules if k == "feelmri" or k.startswith("feelmri.")]:
+            del sys.modules[k]
+        sys.modules.update(saved)
+        feelmri_b200._PATCHES.clear()
+
+
+def test_gather_data_reduces_host_data_on_cuda_under_nccl():
+    # NCCL reduces CUDA tensors only: host (numpy) data must be staged on the
+    # current CUDA device; gloo reduces in place on the host
+    from feelmri_b200.distributed import reduce_device
+    host = torch.zeros(4)
+    assert reduce_device("nccl", host, current_cuda=3) == torch.device("cuda", 3)
+    assert reduce_device("gloo", host) == torch.device("cpu")
+    dev_t = torch.empty(0, device="meta")
+    assert reduce_device("nccl", dev_t, current_cuda=0) == torch.device("cuda", 0)

@@ -3,9 +3,12 @@
 fm_bloch_solve_f32_noalloc serves callers that may not allocate device
 memory: its per-step scratch is a fixed array inside the library instead of
 a workspace the caller allocates.  Both entry points are called here through
-the C ABI on the same inputs, twice in a row with different inputs (the
-shared array keeps the previous call's contents, which must not leak into
-the next result).  This file is collected last so that a run stopping at
+the C ABI on the same inputs, twice in a row with different inputs: first
+with a 4-mode POD motion (the larger weights region), then without motion,
+so that the previous call's contents are still in the shared array when the
+second call runs.  Both entry points run the same kernels on the same inputs
+and differ only in where the scratch lives, so the outputs must be equal bit
+for bit.  This file is collected last so that a run stopping at
 the first failure has run every other test; it also passes on its own.
 """
 import ctypes as C
@@ -59,7 +62,7 @@ def test_no_alloc_matches_workspace_entry_point_twice(cuda):
     N, n_t = 3000, 120
     for call, seed in enumerate((1, 2)):
         d = _inputs(torch, dev, N, n_t, seed)
-        pod = W.sinusoidal_pod(N, n_modes=4, amp=1e-3, period=3.0, n_frames=6) if call == 1 else None
+        pod = W.sinusoidal_pod(N, n_modes=4, amp=1e-3, period=3.0, n_frames=6) if call == 0 else None
         motion = lower(pod, N, dev)
         ref_m = torch.empty((n_t, N), dtype=torch.complex64, device=dev)
         ref_z = torch.empty((n_t, N), dtype=torch.float32, device=dev)
@@ -76,9 +79,8 @@ def test_no_alloc_matches_workspace_entry_point_twice(cuda):
         rm, rz = ref_m.cpu().numpy(), ref_z.cpu().numpy()
         gm, gz = got_m.cpu().numpy(), got_z.cpu().numpy()
         assert np.all(np.isfinite(gm)) and np.all(np.isfinite(gz)), f"call {call}: outputs not written"
-        rel_m = np.linalg.norm(gm - rm) / np.linalg.norm(rm)
-        rel_z = np.linalg.norm(gz - rz) / np.linalg.norm(rz)
-        assert rel_m < 1e-6 and rel_z < 1e-6, (call, rel_m, rel_z)
+        assert np.array_equal(gm, rm), f"call {call}: Mxy differs from the workspace entry point"
+        assert np.array_equal(gz, rz), f"call {call}: Mz differs from the workspace entry point"
 
 
 def test_no_alloc_rejects_oversized_requests(cuda):
