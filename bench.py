@@ -313,7 +313,11 @@ def run_batching(args) -> dict | None:
     bloch_all()
     torch.cuda.synchronize(dev)
     t1 = time.perf_counter()
-    tuning, tried = autotune.tune(problems, force=True)
+    if args.tuning:
+        sn, kc = (int(x) for x in args.tuning.split("/"))
+        tuning, tried = ops.Tuning(split_nodes=sn, kz_cap=kc), {}
+    else:
+        tuning, tried = autotune.tune(problems, force=True)
     tune_s = time.perf_counter() - t1
     batch = ops.SignalBatch(problems, tuning)
 
@@ -1322,6 +1326,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=3.0)
     ap.add_argument("--f32-steps", type=int, default=5, help="batching: timed steps of the FP32 form")
+    ap.add_argument("--tuning", default=None, help="batching: split_nodes/kz_cap instead of the autotuner")
     ap.add_argument("--workload", default="batching",
                     choices=["batching", "plain", "phase_contrast", "precision", "serving", "sequence", "pod",
                              "recon", "node_partition"])

@@ -206,10 +206,15 @@ __device__ __forceinline__ void bloch_segment(const BlochDev &p, BlochNode<RMAX>
   const float *wrow = (MODE == 4) ? p.weights + call0 * p.md.slots + p.md.slot0[p.pod_term] : nullptr;
   const float M0 = p.M0;
   if (flags & kSegDt) {
+    // e1, e2 = exp(-dt / T) rounded once to float (the float64 exponential
+    // of the float32 product, then one rounding), as a correctly rounded
+    // host expf gives them.  (1 - e1) M0 cancels all but a few digits of e1
+    // when dt << T1, so an ulp of difference in e1 would be amplified by
+    // T1 / dt in the recovery; once per segment, so the cost is nil.
     const float dtw = sb->w;
-    s.e1 = expf(__fmul_rn(-dtw, s.invT1));
+    s.e1 = __double2float_rn(exp((double)__fmul_rn(-dtw, s.invT1)));
     s.rec = (1.f - s.e1) * M0;
-    s.e2 = expf(__fmul_rn(-dtw, s.invT2));
+    s.e2 = __double2float_rn(exp((double)__fmul_rn(-dtw, s.invT2)));
   }
   float2 mxy = s.mxy;
   float mz = s.mz;
@@ -223,6 +228,9 @@ __device__ __forceinline__ void bloch_segment(const BlochDev &p, BlochNode<RMAX>
     // mantissa); below |Bz| = 1e-18 both forms clamp to 1e-12 (Bz = 0 on
     // gradient-free steps included); an overflowing square gives +inf and
     // a NaN stays NaN in both.
+    // unrolled: the position, Bz and sin/cos of the next steps do not
+    // depend on this step's magnetisation, so they overlap its update
+#pragma unroll 4
     for (int i = 0; i < count; ++i, ++sa, ++sb) {
       const float aw = sa->w;
       const float4 b = *sb;
@@ -253,6 +261,7 @@ __device__ __forceinline__ void bloch_segment(const BlochDev &p, BlochNode<RMAX>
       }
     }
   } else {
+#pragma unroll 4
     for (int i = 0; i < count; ++i, ++sa, ++sb) {
       const float4 a = *sa;
       const float4 b = *sb;

@@ -80,9 +80,12 @@ struct TcRun {
   int start, P, Q, factored;
 };
 // A work item: rows p0.. and columns q0.. of run `run`, or (nrun > 1) the
-// whole slabs of runs run .. run + nrun - 1 stacked block-diagonally: rows
-// r P + p and column pairs r Q VG + j belong to run `run + r`, and only the
-// diagonal blocks of the product are read.
+// whole slabs of runs run .. run + nrun - 1 stacked along the rows: row
+// r P + p is line p of run `run + r`, and every run shares the columns.
+// The runs then differ only in their times, so each run's decay and
+// off-resonance factor D_r(n) = exp(-t_r / T2_n) exp(i phi_n t_r) moves into
+// its A rows (A = exp(-2 pi i kp . r) D_r) and B = exp(-2 pi i kq . r) (M Mxy)
+// is the same for all of them: the whole product is read.
 struct TcItem {
   int run, p0, q0, nrun;
 };
@@ -101,7 +104,8 @@ struct TcDev {
   const TcRun *runs;
   const TcItem *items;
   int Qt, NT, kind;  // kind 0: factored runs, 1: generic runs
-  int wrows;         // weight rows per node buffer: VG, or (stacked runs) nrun VG
+  int wrows;         // rows per node buffer: VG weight rows, then (stacked runs) nrun D rows
+  int stacked;       // items hold several runs (D in the A rows, B without decay)
   int mm_ld;         // row stride of MM (float2): this group's columns, padded to even
   int tma;           // node blocks are staged by bulk copies (aligned inputs, room in smem)
   const int *plan;  // device: [2] factored items, [3] generic items, [4] splits, [5] nodes per split
@@ -226,7 +230,7 @@ struct TcUnit {
   TcItem it;
   TcRun run;  // the first run
   int split, P_tile, Q_tile, n_stages, n_groups;
-  int rows, pairs;  // active A rows (nrun P_tile) and column pairs (nrun Q_tile VG)
+  int rows, pairs;  // active A rows (nrun P_tile) and column pairs (Q_tile VG)
   int64_t n_begin, n_end;
 };
 
@@ -239,7 +243,7 @@ __device__ inline TcUnit tc_unit(const TcDev &p, const TcWork &W, int u) {
   U.P_tile = min(kTcRows, U.run.P - U.it.p0);
   U.Q_tile = min(p.Qt, U.run.Q - U.it.q0);
   U.rows = U.it.nrun * U.P_tile;
-  U.pairs = U.it.nrun * U.Q_tile * p.VG;
+  U.pairs = U.Q_tile * p.VG;
   U.n_begin = (int64_t)U.split * W.chunk;
   U.n_end = min(p.N, U.n_begin + W.chunk);
   U.n_stages = U.n_end > U.n_begin ? (int)ceil_div(U.n_end - U.n_begin, kTcNodes) : 0;
@@ -366,24 +370,34 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
     pos[2 * kTcBlockNodes + slot] = (double)z;
     // |x| + |y| + |z| for the phase range check (a NaN counts as too large)
     tc_note_max(rmax, __float_as_int(fabsf(x) + fabsf(y) + fabsf(z)) & 0x7fffffff);
-    // one weight set per run of the unit (stacked runs share positions)
-    for (int k = 0; k < U.it.nrun; ++k) {
-      const float tg = (float)p.run_t[U.it.run + k];
+    if (p.stacked) {
+      // the weights without decay (B), then one D_r = decay e^{i phi t_r} row per run (A)
+#pragma unroll
+      for (int v = 0; v < kTcVGroup; ++v)
+        if (v < p.VG) wblk[v * kWStride + slot] = r.m[v];
+      for (int k = 0; k < U.it.nrun; ++k) {
+        const float tg = (float)p.run_t[U.it.run + k];
+        const float decay = expf(-tg * (1.0f / r.t2));
+        float so, co;
+        sincosf(r.phi * tg, &so, &co);
+        wblk[(p.VG + k) * kWStride + slot] = make_float2(decay * co, decay * so);
+      }
+    } else {
+      const float tg = (float)p.run_t[U.it.run];
       const float decay = expf(-tg * (1.0f / r.t2));
       float so, co;
       sincosf(r.phi * tg, &so, &co);
       const float er = decay * co, ei = decay * so;
-      float2 *wk = wblk + k * p.VG * kWStride;
 #pragma unroll
       for (int v = 0; v < kTcVGroup; ++v)
         if (v < p.VG)
-          wk[v * kWStride + slot] = make_float2(r.m[v].x * er - r.m[v].y * ei, r.m[v].x * ei + r.m[v].y * er);
+          wblk[v * kWStride + slot] = make_float2(r.m[v].x * er - r.m[v].y * ei, r.m[v].x * ei + r.m[v].y * er);
     }
   } else {
     pos[slot] = 0.0;
     pos[kTcBlockNodes + slot] = 0.0;
     pos[2 * kTcBlockNodes + slot] = 0.0;
-    for (int v = 0; v < U.it.nrun * p.VG; ++v) wblk[v * kWStride + slot] = make_float2(0.f, 0.f);
+    for (int v = 0; v < p.wrows; ++v) wblk[v * kWStride + slot] = make_float2(0.f, 0.f);
   }
 }
 
@@ -502,7 +516,7 @@ __device__ inline void tc_final(const TcDev &p, int acc_cols, const TcWork &W, c
   const int NH = p.NT >> 1;
   const bool row_ok = row < U.rows;
   float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
-  // row r P_tile + pl belongs to run `run + r`; only that run's column block is read
+  // row r P_tile + pl is line pl of run `run + r`; every run shares the column pairs
   const int r_row = row_ok ? row / U.P_tile : 0, pl = row_ok ? row % U.P_tile : 0;
   const int qvg = U.Q_tile * p.VG;
   const int start = row_ok ? p.runs[U.it.run + r_row].start : 0;
@@ -525,10 +539,9 @@ __device__ inline void tc_final(const TcDev &p, int acc_cols, const TcWork &W, c
         re = __uint_as_float(sr[i]) + re;
         im = __uint_as_float(sm[i]) + im;
       }
-      const int jj = c0 + i;  // pair (run block, q, v)
-      if (jj / qvg != r_row) continue;
-      const int jv = jj % qvg;
-      const int q = jv / p.VG, vv = jv % p.VG;
+      const int jj = c0 + i;  // pair (q, v)
+      if (jj >= qvg) continue;
+      const int q = jj / p.VG, vv = jj % p.VG;
       if (q < U.Q_tile) dst[(int64_t)(s_row + q) * p.V + p.v0 + vv] = make_float2(re, im);
     }
   }
@@ -646,10 +659,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     // per-unit row data in registers
     double kx0 = 0, ky0 = 0, kz0 = 0, kx1 = 0, ky1 = 0, kz1 = 0;  // A: kp of the row; B: kq of q and q + 32
     int bq = 0, bw = 0;  // B: phase-table row and weight row of the pair
+    int a_drow = 0;      // A of a stacked unit: the row's D row in the node buffer
     if (a_role) {
       if (row < U.rows) {
         // row r P_tile + pl belongs to run `run + r` (r = 0 unless stacked)
         const int r = row / U.P_tile, pl = row % U.P_tile;
+        a_drow = VG + r;
         const int start = r == 0 ? U.run.start : p.runs[U.it.run + r].start;
         const int s_p = start + (fac ? (U.it.p0 + pl) * p.n_kz : U.it.p0 + pl);
         kx0 = p.kx[s_p];
@@ -659,10 +674,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       }
     } else {
       if (row < U.pairs) {
-        const int qvg = U.Q_tile * VG;
-        const int r = row / qvg, jv = row % qvg;
-        bq = jv / VG;
-        bw = r * VG + jv % VG;
+        bq = row / VG;
+        bw = row % VG;
       }
       if (fac) {
         const int s_0 = U.run.start;
@@ -804,20 +817,39 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           if (st >= s_end) break;
           const uint32_t s = (g0 + st) & (kTcStages - 1), j = jg + i;
           if (active) {
-            // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n
+            // A'[row][2n..2n+1] = (Re A, -Im A) = (cos, sin) of 2 pi kp . r_n;
+            // in a stacked unit A is multiplied by the row's run factor D_r(n):
+            // (Re, -Im) of (cos - i sin)(dr + i di) = (cos dr + sin di, sin dr - cos di)
             const uint32_t stg = sstages + s * L.stage_bytes;
             const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 8 * half;
             uint32_t h[8], l[8];
+            if (p.stacked) {
+              const float4 *dp = reinterpret_cast<const float4 *>(w_all + (buf * WR + a_drow) * kWStride +
+                                                                  j * kTcNodes + 8 * half);
 #pragma unroll
-            for (int u4 = 0; u4 < 8; u4 += 2) {
-              const double2 x = *reinterpret_cast<const double2 *>(px + u4);
-              const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
-              const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
-              float c0, s0, c1, s1;
-              cycles_cos_sin(fma(kz0, z.x, fma(ky0, y.x, kx0 * x.x)), c0, s0);
-              cycles_cos_sin(fma(kz0, z.y, fma(ky0, y.y, kx0 * x.y)), c1, s1);
-              split_pair(c0, s0, h[u4], l[u4]);
-              split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
+              for (int u4 = 0; u4 < 8; u4 += 2) {
+                const double2 x = *reinterpret_cast<const double2 *>(px + u4);
+                const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
+                const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
+                float c0, s0, c1, s1;
+                cycles_cos_sin(fma(kz0, z.x, fma(ky0, y.x, kx0 * x.x)), c0, s0);
+                cycles_cos_sin(fma(kz0, z.y, fma(ky0, y.y, kx0 * x.y)), c1, s1);
+                const float4 d = dp[u4 >> 1];
+                split_pair(fmaf(c0, d.x, s0 * d.y), fmaf(s0, d.x, -(c0 * d.y)), h[u4], l[u4]);
+                split_pair(fmaf(c1, d.z, s1 * d.w), fmaf(s1, d.z, -(c1 * d.w)), h[u4 + 1], l[u4 + 1]);
+              }
+            } else {
+#pragma unroll
+              for (int u4 = 0; u4 < 8; u4 += 2) {
+                const double2 x = *reinterpret_cast<const double2 *>(px + u4);
+                const double2 y = *reinterpret_cast<const double2 *>(px + kTcBlockNodes + u4);
+                const double2 z = *reinterpret_cast<const double2 *>(px + 2 * kTcBlockNodes + u4);
+                float c0, s0, c1, s1;
+                cycles_cos_sin(fma(kz0, z.x, fma(ky0, y.x, kx0 * x.x)), c0, s0);
+                cycles_cos_sin(fma(kz0, z.y, fma(ky0, y.y, kx0 * x.y)), c1, s1);
+                split_pair(c0, s0, h[u4], l[u4]);
+                split_pair(c1, s1, h[u4 + 1], l[u4 + 1]);
+              }
             }
             const uint32_t a_st = stg + o_hi;
             st_shared_v4(a_st, h[0], h[1], h[2], h[3]);
@@ -852,7 +884,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           const uint32_t s = (g0 + st) & (kTcStages - 1), j = jg + i;
           // B'^T rows: re row `row` = (Re B, Im B), im row NT/2 + row =
           // (Im B, -Re B), B = e_q(n) W'(n, v).  Pairs past Q_tile VG hold
-          // values no output reads.
+          // values no output reads.  Threads past the tile's NT/2 pairs have
+          // no B element (their warps only take part in the phase table).
+          if (b_rows) {
           const float4 *wp =
               reinterpret_cast<const float4 *>(w_all + (buf * WR + bw) * kWStride + j * kTcNodes + 8 * half);
           float br[8], bi[8];
@@ -881,7 +915,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
             hm[i] = __byte_perm(hr[i], 0u, 0x1032) ^ 0x80000000u;
             lm[i] = __byte_perm(lr[i], 0u, 0x1032) ^ 0x80000000u;
           }
-          if (b_rows) {
+          {
             const uint32_t stg = sstages + s * L.stage_bytes;
             const uint32_t b_st = stg + o_hi;
             st_shared_v4(b_st, hr[0], hr[1], hr[2], hr[3]);
@@ -893,6 +927,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
             st_shared_v4(b_st + d_im + d_lo, lm[0], lm[1], lm[2], lm[3]);
             st_shared_v4(b_st + d_im + d_lo + 128, lm[4], lm[5], lm[6], lm[7]);
           }
+          }  // b_rows
           // the phase table of stage st + kTcFacGroup (next group) into its
           // buffer, whose last readers (stage st - kTcFacGroup) are past the
           // previous group's barrier
@@ -1261,23 +1296,19 @@ static int tc_qt(const fm_signal_args *a, int VG, const fm_tc_tuning *tune) {
 }
 
 // Runs per stacked unit for a column group: whole slabs only (lines <= 128
-// rows, kz within one tile), at most 128 rows, 128 column pairs and 8 weight
-// rows, and only without motion (the runs then share node positions).
+// rows, kz within one tile), at most 128 rows (kTcMaxStack runs), and only
+// without motion (the runs then share node positions).  The node buffers
+// hold the VG weight rows and one D row per run.
+constexpr int kTcMaxStack = 16;
 static int tc_stack_runs(const fm_signal_args *a, int VG, int Qt) {
   if (a->motion && a->motion->kind != FM_MOTION_NONE) return 1;
   if (a->n_kz < 2 || a->n_lines * a->n_kz < 2 || a->n_kz > Qt || a->n_lines > kTcRows) return 1;
   int R = kTcRows / (int)a->n_lines;
-  const int by_pairs = kTcRows / (int)(a->n_kz * VG);
-  const int by_weights = kTcVGroup / VG;
-  if (by_pairs < R) R = by_pairs;
-  if (by_weights < R) R = by_weights;
-  // the stacked unit's tiles and weight rows must fit in shared memory
-  while (R > 1) {
-    int NT, acc;
-    tc_shape(Qt, R * VG, NT, acc);
-    if (tc_smem_layout(NT, R * VG, Qt).total <= kTcSmemMax) break;
-    --R;
-  }
+  if (R > kTcMaxStack) R = kTcMaxStack;
+  // the tiles and node buffers must fit in shared memory
+  int NT, acc;
+  tc_shape(Qt, VG, NT, acc);
+  while (R > 1 && tc_smem_layout(NT, VG + R, Qt).total > kTcSmemMax) --R;
   return R < 2 ? 1 : R;
 }
 
@@ -1389,11 +1420,12 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
       p.error = pl.runs.error;
       p.kind = kind;
       p.Qt = kind == 0 ? Qt_f : 1;
-      // a stacked unit holds R runs' columns and weight rows
+      // a stacked unit's node buffers add one D row per run
       const int Rk = kind == 0 ? R : 1;
-      p.wrows = Rk * VG;
+      p.stacked = Rk > 1 ? 1 : 0;
+      p.wrows = VG + (Rk > 1 ? Rk : 0);
       int acc_cols;
-      tc_shape(p.Qt, Rk * VG, p.NT, acc_cols);
+      tc_shape(p.Qt, VG, p.NT, acc_cols);
       // node blocks by bulk copies when the inputs are 16-byte aligned and the
       // staging area fits next to the tiles
       const bool aligned = ((uintptr_t)p.r0 % 16 == 0) && ((uintptr_t)p.T2 % 16 == 0) &&
