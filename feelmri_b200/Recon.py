@@ -35,7 +35,7 @@ from . import ops
 from ._motion import lower
 
 __all__ = ["grid_points", "nudft_forward", "nudft_adjoint", "dcf_pipe_menon", "dcf_path_jacobian",
-           "reconstruct_nudft"]
+           "reconstruct_nudft", "cartesian_recon", "CartesianRecon"]
 
 
 def grid_points(img_shape, fov) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
@@ -209,3 +209,87 @@ def reconstruct_nudft(kdata, ktraj, img_shape, fov, *, dcw=None, auto_dcw: str |
     if combine.lower() == "rss":
         return np.sqrt(np.sum(np.abs(img) ** 2, axis=0)).astype(np.complex64)
     raise ValueError(f"unknown combine {combine!r}: use None or 'rss'")
+
+
+# ------------------------------------------------------- Cartesian recon --
+
+def _kspace_window(n: int, kind: str, width: float = 0.9, lift: float = 0.3) -> np.ndarray:
+    """1-D k-space apodisation of length n.  'Tukey': a Tukey window with
+    taper fraction 1 - width, lifted to [lift, 1]; 'Riesz': flat in the
+    middle `width` of the axis, falling as 1 - (1 - lift) (d / d0)^2 over
+    each end stretch of round((1 - width) n / 2) samples (d the distance
+    into the stretch from its inner edge, d0 half the stretch length)."""
+    if kind == "Tukey":
+        from scipy.signal.windows import tukey
+        return tukey(n, alpha=1.0 - width) * (1.0 - lift) + lift
+    if kind == "Riesz":
+        m = int(np.round((1.0 - width) / 2 * n))
+        h = np.ones(n)
+        if m > 0:
+            d = np.linspace(0.0, m / 2, m)
+            edge = 1.0 - (np.abs(d / (m / 2)) ** 2) * (1.0 - lift)
+            h[:m] *= edge[::-1]
+            h[n - m:] *= edge
+        return h
+    return np.ones(n)
+
+
+def cartesian_recon(K, trajectory, filter=None) -> np.ndarray:
+    """Image from Cartesian k-space by the inverse FFT on the GPU, with the
+    steps of CartesianRecon (python/feelmri/Recon.py:13-90):
+
+    * for a CartesianStack with several lines per shot, lines read in the
+      reverse direction (odd positions within their shot) are flipped along
+      the readout;
+    * axes 0-2 with an even resolution are zero-padded by one sample at the
+      end (so that the image is not shifted);
+    * the k-space is apodised along the readout and phase axes by a Tukey or
+      Riesz window (width 0.9, lift 0.3, as the reference fixes them; any
+      other filter type applies none);
+    * the centred inverse FFT over axes 0-2 (torch.fft on the device);
+    * the image is brought to oversampling x res along the first three axes
+      by trilinear interpolation when the shapes differ, then the readout is
+      cut to res[0] around its centre.
+
+    K: (n_ro, n_lines, n_kz, ...) complex; trajectory: an object with .res,
+    .oversampling_arr and, for line reordering, .lines_per_shot and .shots
+    (the reference's CartesianStack attributes).  Returns complex64 of shape
+    (res[0], res[1], res[2], ...) (the reference's interpolation differs
+    in detail when shapes change: skimage's resize, not available here)."""
+    dev = ops.require_cuda()
+    kind = (filter or {"type": "Tukey"}).get("type")
+    K = np.array(K, dtype=np.complex64, copy=True)
+    if K.ndim < 3:
+        raise ValueError(f"K must have at least 3 dimensions (readout, lines, kz), got {K.shape}")
+    extra = K.shape[3:]
+    res = np.asarray(trajectory.res).astype(int)
+    lps = int(getattr(trajectory, "lines_per_shot", 1) or 1)
+    if lps > 1:
+        for shot in getattr(trajectory, "shots", []):
+            for pos, line in enumerate(shot):
+                if pos % 2 == 1 and line is not None:
+                    K[:, line] = K[::-1, line].copy()
+    pad = [(0, 1) if res[d] % 2 == 0 else (0, 0) for d in range(3)] + [(0, 0)] * len(extra)
+    if any(p != (0, 0) for p in pad):
+        K = np.pad(K, pad)
+    h = np.outer(_kspace_window(K.shape[0], kind), _kspace_window(K.shape[1], kind)).astype(np.float32)
+    t = torch.from_numpy(K).to(dev)
+    t = t * torch.from_numpy(h).to(dev).reshape(h.shape + (1,) * (K.ndim - 2))
+    dims = (0, 1, 2)
+    img = torch.fft.fftshift(torch.fft.ifftn(torch.fft.ifftshift(t, dim=dims), dim=dims), dim=dims)
+    target = tuple(int(round(x)) for x in np.asarray(trajectory.oversampling_arr) * res)
+    if tuple(img.shape[:3]) != target:
+        flat = img.reshape(img.shape[:3] + (-1,)).permute(3, 0, 1, 2)  # (C, X, Y, Z)
+        parts = [torch.nn.functional.interpolate(part.unsqueeze(0), size=target, mode="trilinear",
+                                                 align_corners=False)[0]
+                 for part in (flat.real.contiguous(), flat.imag.contiguous())]
+        img = torch.complex(parts[0], parts[1]).permute(1, 2, 3, 0).reshape(target + extra)
+    enc, rec = img.shape[0], int(res[0])
+    if enc != rec:
+        a = (enc - rec) // 2
+        img = img[a:a + rec]
+    return ops.to_host(img.contiguous())
+
+
+# the reference's name for the same call
+CartesianRecon = cartesian_recon

@@ -185,12 +185,17 @@ __host__ __device__ inline uint32_t tc_raw_bytes(int mm_ld) {
   return kTcBlockNodes * (12 + 4 + 4 + 8 * mm_ld);
 }
 
-// Byte offset of element (row, k) of a K-major, no-swizzle operand tile with
-// `rows` rows and 32 K elements: two K steps of 16, each made of 8-row x
-// 16-byte core matrices (LBO = 128 between K halves, SBO = 256 between row
-// groups).
-__host__ __device__ inline uint32_t kmajor_offset(uint32_t row, uint32_t k, uint32_t rows) {
-  return (k >> 4) * (rows * 32) + (row >> 3) * 256 + ((k >> 3) & 1) * 128 + (row & 7) * 16 + (k & 7) * 2;
+// Byte offset of element (row, k) of a K-major operand tile with 32 K
+// elements (64-byte rows) in the 64-byte swizzled layout: row r at r * 64,
+// its 16-byte chunk c (elements 8c .. 8c + 7) stored at chunk position
+// c ^ ((r >> 1) & 3), i.e. address bits 4-5 XOR bits 7-8.  Tiles start on
+// 512-byte boundaries (8-row groups, SBO = 512), so the swizzle of a byte
+// offset is the swizzle of its shared-memory address.  The tensor core reads
+// this layout at full shared-memory bandwidth; the unswizzled layout's
+// 16-byte core-matrix rows cap its operand reads, which dominates narrow
+// (small N) MMAs.
+__host__ __device__ inline uint32_t sw64_offset(uint32_t row, uint32_t k) {
+  return row * 64 + ((((k >> 3) ^ (row >> 1)) & 3) << 4) + (k & 7) * 2;
 }
 
 // hi = bf16(x), lo = bf16(x - hi) for the pair (a, b); bits of (hi_a, hi_b)
@@ -370,6 +375,11 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
     pos[2 * kTcBlockNodes + slot] = (double)z;
     // |x| + |y| + |z| for the phase range check (a NaN counts as too large)
     tc_note_max(rmax, __float_as_int(fabsf(x) + fabsf(y) + fabsf(z)) & 0x7fffffff);
+    // decay exp(-t / T2) and off-resonance rotation exp(i phi t) of a run:
+    // the fast exponential of -t (1 / T2), and the phase phi t reduced in
+    // cycles in FP64 before the fast sin/cos (cycles_cos_sin), as the A and B
+    // tiles do (both within a few 1e-7 of the accurate functions)
+    const float inv_t2 = __frcp_rn(r.t2);
     if (p.stacked) {
       // the weights without decay (B), then one D_r = decay e^{i phi t_r} row per run (A)
 #pragma unroll
@@ -377,16 +387,16 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
         if (v < p.VG) wblk[v * kWStride + slot] = r.m[v];
       for (int k = 0; k < U.it.nrun; ++k) {
         const float tg = (float)p.run_t[U.it.run + k];
-        const float decay = expf(-tg * (1.0f / r.t2));
+        const float decay = __expf(-tg * inv_t2);
         float so, co;
-        sincosf(r.phi * tg, &so, &co);
+        cycles_cos_sin((double)(r.phi * tg) * 0.15915494309189535, co, so);
         wblk[(p.VG + k) * kWStride + slot] = make_float2(decay * co, decay * so);
       }
     } else {
       const float tg = (float)p.run_t[U.it.run];
-      const float decay = expf(-tg * (1.0f / r.t2));
+      const float decay = __expf(-tg * inv_t2);
       float so, co;
-      sincosf(r.phi * tg, &so, &co);
+      cycles_cos_sin((double)(r.phi * tg) * 0.15915494309189535, co, so);
       const float er = decay * co, ei = decay * so;
 #pragma unroll
       for (int v = 0; v < kTcVGroup; ++v)
@@ -462,51 +472,66 @@ __device__ inline void tc_phase_pair(const double *pb, float2 *et, int q, int n0
   *reinterpret_cast<float4 *>(et + q * kEStride + n0) = make_float4(c0, -s0, c1, -s1);
 }
 
-// Tensor memory: the accumulator in columns [0, NT) and the FP32 running sum
-// in [acc_cols, acc_cols + NT).  Accumulator column j < NT/2 is the real
-// part of pair j, column NT/2 + j its imaginary part.
+// Tensor memory (all 512 columns of the SM).  Wide tiles (NT > 128): the
+// accumulator in columns [0, NT) collects all three products.  Narrow tiles
+// (NT <= 128): the B hi and lo tiles are contiguous, so one MMA with
+// N = 2 NT gives A_hi B_hi in columns [0, NT) and A_hi B_lo in [NT, 2 NT), and
+// a second MMA adds A_lo B_hi into [0, NT): two MMAs per K step instead of
+// three.  A narrow tile's MMAs cost about as much as wide ones to issue
+// (the tensor core takes ~45 cycles per MMA at N <= 64 against 128 at
+// N = 256), so their count, not their size, sets the pace.  The FP32 running
+// sum follows at column sum_col.  In each part, column j < NT/2 is the real
+// part of pair j and column NT/2 + j its imaginary part.
+constexpr uint32_t kTcTmemCols = 512;
+__host__ __device__ inline bool tc_narrow(int NT) { return NT <= 128; }
+__host__ __device__ inline int tc_parts(int NT) { return tc_narrow(NT) ? 2 : 1; }
+__host__ __device__ inline int tc_sum_col(int NT) { return ((tc_parts(NT) * NT) + 31) & ~31; }
 
 // Folds the accumulator (group gg, complete once accfull's phase gg & 1
-// has flipped) into the running sum: sum = acc (first group) or sum + acc,
-// in FP32 round-to-nearest.  Warp w handles TMEM lanes of quarter w % 4 and
-// column quarter w / 4.  The next MMA into the accumulator is issued after a
-// block barrier.
-__device__ inline void tc_fold(const TcDev &p, int acc_cols, uint64_t *accfull, uint32_t tmem, int gg, bool first,
+// has flipped) into the running sum: sum = part_0 (+ part_1) for the first
+// group, else sum + (part_0 (+ part_1)), in FP32 round-to-nearest.  Warp w
+// handles TMEM lanes of quarter w % 4 and column quarter w / 4.  The next MMA
+// into the accumulator is issued after a block barrier.
+__device__ inline void tc_fold(const TcDev &p, uint64_t *accfull, uint32_t tmem, int gg, bool first,
                                volatile int *abort_flag) {
   const int warp = threadIdx.x >> 5;
   tc_wait(accfull, gg & 1, abort_flag);
   ptx::tc_fence_after();
+  const int NT = p.NT, n_acc = tc_parts(NT), sum_col = tc_sum_col(NT);
   const int quarter = warp & 3, cq = warp >> 2;
-  const int cpq = ((p.NT / 4 + 15) / 16) * 16;
-  const int c_begin = cq * cpq, c_end = min(p.NT, c_begin + cpq);
+  const int cpq = ((NT / 4 + 15) / 16) * 16;
+  const int c_begin = cq * cpq, c_end = min(NT, c_begin + cpq);
   const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
   for (int c0 = c_begin; c0 < c_end; c0 += 16) {
     uint32_t a[16];
     ptx::tmem_ld16(tmem + lanes + (uint32_t)c0, a);
-    if (!first) {
-      // the running sum in two halves of 8 columns (fewer live registers)
-      uint32_t r[8];
+    ptx::tmem_wait_ld();
+    // the other accumulators, then the running sum, in halves of 8 columns
+    for (int k = 1; k <= n_acc; ++k) {
+      if (k == n_acc && first) break;
+      const int col = (k == n_acc ? sum_col : k * NT) + c0;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        ptx::tmem_ld8(tmem + lanes + (uint32_t)(acc_cols + c0 + 8 * h), r);
+        uint32_t r[8];
+        ptx::tmem_ld8(tmem + lanes + (uint32_t)(col + 8 * h), r);
         ptx::tmem_wait_ld();
 #pragma unroll
         for (int i = 0; i < 8; ++i)
-          a[8 * h + i] = __float_as_uint(__uint_as_float(r[i]) + __uint_as_float(a[8 * h + i]));
+          a[8 * h + i] = k == n_acc ? __float_as_uint(__uint_as_float(r[i]) + __uint_as_float(a[8 * h + i]))
+                                    : __float_as_uint(__uint_as_float(a[8 * h + i]) + __uint_as_float(r[i]));
       }
-    } else {
-      ptx::tmem_wait_ld();
     }
-    ptx::tmem_st16(tmem + lanes + (uint32_t)(acc_cols + c0), a);
+    ptx::tmem_st16(tmem + lanes + (uint32_t)(sum_col + c0), a);
   }
   ptx::tmem_wait_st();
   ptx::tc_fence_before();
 }
 
 // Writes the unit's result: running sum (when earlier groups were folded) +
-// accumulator of the last group gg, to the output samples.  Warp w reads TMEM
-// lanes of quarter w % 4 and every fourth chunk of 8 pairs starting at w / 4.
-__device__ inline void tc_final(const TcDev &p, int acc_cols, const TcWork &W, const TcUnit &U, uint64_t *accfull,
+// the accumulator of the last group gg (its parts added in order), to the
+// output samples.  Warp w reads TMEM lanes of quarter w % 4 and every fourth
+// chunk of 8 pairs starting at w / 4.
+__device__ inline void tc_final(const TcDev &p, const TcWork &W, const TcUnit &U, uint64_t *accfull,
                                 uint32_t tmem, int gg, bool has_sum, volatile int *abort_flag) {
   const int tid = threadIdx.x, warp = tid >> 5;
   tc_wait(accfull, gg & 1, abort_flag);
@@ -522,23 +547,42 @@ __device__ inline void tc_final(const TcDev &p, int acc_cols, const TcWork &W, c
   const int start = row_ok ? p.runs[U.it.run + r_row].start : 0;
   const int s_row = start + (U.run.factored ? (U.it.p0 + pl) * p.n_kz + U.it.q0 : U.it.p0 + pl);
   const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
+  const int n_acc = tc_parts(p.NT), AW = p.NT, sum_col = tc_sum_col(p.NT);
   for (int c0 = (warp >> 2) * 8; c0 < NH; c0 += 32) {
-    uint32_t r[8], m[8], sr[8], sm[8];
+    uint32_t r[8], m[8];
     ptx::tmem_ld8(taddr + (uint32_t)c0, r);
     ptx::tmem_ld8(taddr + (uint32_t)(NH + c0), m);
-    if (has_sum) {
-      ptx::tmem_ld8(taddr + (uint32_t)(acc_cols + c0), sr);
-      ptx::tmem_ld8(taddr + (uint32_t)(acc_cols + NH + c0), sm);
-    }
     ptx::tmem_wait_ld();
+    float re8[8], im8[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      re8[i] = __uint_as_float(r[i]);
+      im8[i] = __uint_as_float(m[i]);
+    }
+    for (int k = 1; k < n_acc; ++k) {
+      ptx::tmem_ld8(taddr + (uint32_t)(k * AW + c0), r);
+      ptx::tmem_ld8(taddr + (uint32_t)(k * AW + NH + c0), m);
+      ptx::tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        re8[i] = re8[i] + __uint_as_float(r[i]);
+        im8[i] = im8[i] + __uint_as_float(m[i]);
+      }
+    }
+    if (has_sum) {
+      ptx::tmem_ld8(taddr + (uint32_t)(sum_col + c0), r);
+      ptx::tmem_ld8(taddr + (uint32_t)(sum_col + NH + c0), m);
+      ptx::tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        re8[i] = __uint_as_float(r[i]) + re8[i];
+        im8[i] = __uint_as_float(m[i]) + im8[i];
+      }
+    }
     if (!row_ok) continue;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      float re = __uint_as_float(r[i]), im = __uint_as_float(m[i]);
-      if (has_sum) {
-        re = __uint_as_float(sr[i]) + re;
-        im = __uint_as_float(sm[i]) + im;
-      }
+      const float re = re8[i], im = im8[i];
       const int jj = c0 + i;  // pair (q, v)
       if (jj >= qvg) continue;
       const int q = jj / p.VG, vv = jj % p.VG;
@@ -552,26 +596,46 @@ __device__ inline void tc_final(const TcDev &p, int acc_cols, const TcWork &W, c
 // n_stages stages): A_hi B_hi + A_hi B_lo + A_lo B_hi over the two K steps
 // into the accumulator (overwritten at a group's first stage); the stage's
 // shared memory is released by a commit to empty[s], and the group's
-// accumulator by a commit to accfull after the group's last stage.
+// accumulator by a commit to accfull after the group's last stage.  Called by
+// the whole issuing warp (warp 7): the descriptors are warp-uniform, and
+// lane 0 issues the MMAs and commits (it is the thread whose operations the
+// commits track).
 __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, uint32_t idesc, int NT,
-                                uint64_t *empty, uint64_t *accfull, uint32_t g, uint32_t st, uint32_t n_stages) {
+                                uint64_t *empty, uint64_t *accfull, uint32_t g, uint32_t st, uint32_t n_stages,
+                                uint32_t lane) {
   const uint32_t s = g % kTcStages;
-  const bool group_start = (st % kTcDrain) == 0;
   ptx::tc_fence_after();
   const uint32_t stage = sbase + L.stages + s * L.stage_bytes;
-  const uint32_t acc = tmem;
+  // the drain group's first stage overwrites the accumulator; everything is
+  // computed before the first MMA goes out
+  const uint32_t acc0 = (st % kTcDrain) == 0 ? 0u : 1u;
+  uint64_t ad[2][2], bd[2][2];
 #pragma unroll
   for (int ks = 0; ks < 2; ++ks) {
-    const uint64_t ah = ptx::smem_desc(stage + L.a_hi + ks * kTcRows * 32, 128, 256);
-    const uint64_t al = ptx::smem_desc(stage + L.a_lo + ks * kTcRows * 32, 128, 256);
-    const uint64_t bh = ptx::smem_desc(stage + L.b_hi + ks * NT * 32, 128, 256);
-    const uint64_t bl = ptx::smem_desc(stage + L.b_lo + ks * NT * 32, 128, 256);
-    ptx::mma_bf16(acc, ah, bh, idesc, (group_start && ks == 0) ? 0u : 1u);
-    ptx::mma_bf16(acc, ah, bl, idesc, 1u);
-    ptx::mma_bf16(acc, al, bh, idesc, 1u);
+    // K step ks: elements 16 ks .. 16 ks + 15, bytes 32 ks .. of every row
+    ad[ks][0] = ptx::smem_desc_sw64(stage + L.a_hi + ks * 32);
+    ad[ks][1] = ptx::smem_desc_sw64(stage + L.a_lo + ks * 32);
+    bd[ks][0] = ptx::smem_desc_sw64(stage + L.b_hi + ks * 32);
+    bd[ks][1] = ptx::smem_desc_sw64(stage + L.b_lo + ks * 32);
   }
-  ptx::mma_commit(&empty[s]);
-  if ((st % kTcDrain) == kTcDrain - 1 || st == n_stages - 1) ptx::mma_commit(accfull);
+  if (tc_narrow(NT)) {
+    // A_hi [B_hi; B_lo] (N = 2 NT, both tiles from b_hi on), then A_lo B_hi
+    const uint32_t idesc2 = ptx::idesc_bf16_f32(kTcRows, 2 * NT);
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) {
+      ptx::mma_bf16_lane0(tmem, ad[ks][0], bd[ks][0], idesc2, ks == 0 ? acc0 : 1u, lane);
+      ptx::mma_bf16_lane0(tmem, ad[ks][1], bd[ks][0], idesc, 1u, lane);
+    }
+  } else {
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) {
+      ptx::mma_bf16_lane0(tmem, ad[ks][0], bd[ks][0], idesc, ks == 0 ? acc0 : 1u, lane);
+      ptx::mma_bf16_lane0(tmem, ad[ks][0], bd[ks][1], idesc, 1u, lane);
+      ptx::mma_bf16_lane0(tmem, ad[ks][1], bd[ks][0], idesc, 1u, lane);
+    }
+  }
+  ptx::mma_commit_lane0(&empty[s], lane);
+  if ((st % kTcDrain) == kTcDrain - 1 || st == n_stages - 1) ptx::mma_commit_lane0(accfull, lane);
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_constant__ TcBatchDev B) {
@@ -604,7 +668,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     *rmax = 0;
     ptx::fence_mbar_init();
   }
-  if (warp == 0) ptx::tmem_alloc(tmem_slot, 2 * B.acc_cols);
+  if (warp == 0) ptx::tmem_alloc(tmem_slot, kTcTmemCols);
   ptx::tc_fence_before();
   __syncthreads();
   ptx::tc_fence_after();
@@ -622,7 +686,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   const int row = (rw >> 1) * 32 + lane;  // A row or B pair
   const int half = rw & 1;                // nodes 8 half .. 8 half + 7 of a stage
   const bool loader = tid < kTcBlockNodes;
-  const bool issuer = tid == 7 * 32;
+  const bool issuer = tid == 7 * 32;  // lane 0 of warp 7: the thread that issues every MMA
   // phase-table thread: q = (tid - 256) / 8 (+ 32), nodes 2 ((tid - 256) % 8) + {0, 1}
   const int tq = (tid - 256) >> 3, tn = ((tid - 256) & 7) * 2;
   uint32_t gst = 0, raw_seq = 0;
@@ -645,12 +709,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     const uint32_t sstages = sbase + L.stages;
     const uint32_t idesc = ptx::idesc_bf16_f32(kTcRows, NT);
     // operand addresses inside a stage: the thread's first 8-K chunk; the
-    // second chunk is 128 bytes on, the lo tile d_lo bytes on and (B) the
-    // imaginary row block d_im bytes on
-    const uint32_t o_hi = a_role ? L.a_hi + kmajor_offset(row, 16 * half, kTcRows)
-                                 : L.b_hi + kmajor_offset(row, 16 * half, NT);
+    // second chunk is d_k2 = +/-16 bytes from it (swizzled chunk positions
+    // 2 half and 2 half + 1 differ in their lowest bit), the lo tile d_lo
+    // bytes on and (B) the imaginary row block d_im bytes on
+    const uint32_t o_hi = (a_role ? L.a_hi : L.b_hi) + sw64_offset(row, 16 * half);
+    const int d_k2 = ((((2 * half) ^ (row >> 1)) & 1) != 0) ? -16 : 16;
     const uint32_t d_lo = a_role ? L.a_lo - L.a_hi : L.b_lo - L.b_hi;
-    const uint32_t d_im = (uint32_t)(NH >> 3) * 256;
+    const uint32_t d_im = (uint32_t)NH * 64;
     const bool b_rows = row < NH;
     const TcUnit U = tc_unit(p, W, u - B.offsets[e_lo]);
     const bool fac = U.run.factored != 0;
@@ -731,12 +796,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         if (nst > 0) tc_note_k(kmax, gx, gy, gz);
       }
       const bool g_active = (warp & 3) * 32 < U.P_tile;
-      const uint32_t ga0 = L.a_hi + kmajor_offset(grow, 8 * gc, kTcRows);
-      const uint32_t gl0 = L.a_lo + kmajor_offset(grow, 8 * gc, kTcRows);
+      const uint32_t ga0 = L.a_hi + sw64_offset(grow, 8 * gc);
+      const uint32_t gl0 = L.a_lo + sw64_offset(grow, 8 * gc);
       const int gpair = tid & 7, gnode = tid >> 3;
       const bool g_b = tid < kTcRows && gpair < NH;
       const int gv = gpair < VG ? gpair : 0;
-      const uint32_t gbr = kmajor_offset(gpair, 2 * gnode, NT), gbi = kmajor_offset(NH + gpair, 2 * gnode, NT);
+      const uint32_t gbr = sw64_offset(gpair, 2 * gnode), gbi = sw64_offset(NH + gpair, 2 * gnode);
       // The MMAs of a generic stage are small (N = 16), so the producers
       // write kTcGenGroup stages between barriers and the issuer sends them
       // together: one barrier per group instead of one per stage.  Groups
@@ -785,12 +850,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         ptx::fence_proxy_async_smem();
         // every writer of the group is done: its MMAs go out now
         ptx::named_barrier(1, kTcProducers);
-        if (issuer)
-          for (uint32_t st = sg; st < s_end; ++st) tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst);
+        if (warp == 7)
+          for (uint32_t st = sg; st < s_end; ++st)
+            tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst, lane);
         // an accumulation group ended with this group: fold it before the
         // next group's MMAs (which go out at the next barrier)
         if (s_end < nst && (s_end & (kTcDrain - 1)) == 0) {
-          tc_fold(p, B.acc_cols, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
+          tc_fold(p, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
       }
@@ -853,21 +919,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
             }
             const uint32_t a_st = stg + o_hi;
             st_shared_v4(a_st, h[0], h[1], h[2], h[3]);
-            st_shared_v4(a_st + 128, h[4], h[5], h[6], h[7]);
+            st_shared_v4(a_st + d_k2, h[4], h[5], h[6], h[7]);
             st_shared_v4(a_st + d_lo, l[0], l[1], l[2], l[3]);
-            st_shared_v4(a_st + d_lo + 128, l[4], l[5], l[6], l[7]);
+            st_shared_v4(a_st + d_lo + d_k2, l[4], l[5], l[6], l[7]);
           }
         }
         ptx::fence_proxy_async_smem();
         // every writer of the group is done (and its phase tables of the next
         // group are visible after this barrier): its MMAs go out now
         ptx::named_barrier(1, kTcProducers);
-        if (issuer)
-          for (uint32_t st = sg; st < s_end; ++st) tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst);
+        if (warp == 7)
+          for (uint32_t st = sg; st < s_end; ++st)
+            tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst, lane);
         // an accumulation group ended with this group: fold it before the
         // next group's MMAs go out
         if (s_end < nst && (s_end & (kTcDrain - 1)) == 0) {
-          tc_fold(p, B.acc_cols, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
+          tc_fold(p, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
       }
@@ -919,13 +986,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
             const uint32_t stg = sstages + s * L.stage_bytes;
             const uint32_t b_st = stg + o_hi;
             st_shared_v4(b_st, hr[0], hr[1], hr[2], hr[3]);
-            st_shared_v4(b_st + 128, hr[4], hr[5], hr[6], hr[7]);
+            st_shared_v4(b_st + d_k2, hr[4], hr[5], hr[6], hr[7]);
             st_shared_v4(b_st + d_lo, lr[0], lr[1], lr[2], lr[3]);
-            st_shared_v4(b_st + d_lo + 128, lr[4], lr[5], lr[6], lr[7]);
+            st_shared_v4(b_st + d_lo + d_k2, lr[4], lr[5], lr[6], lr[7]);
             st_shared_v4(b_st + d_im, hm[0], hm[1], hm[2], hm[3]);
-            st_shared_v4(b_st + d_im + 128, hm[4], hm[5], hm[6], hm[7]);
+            st_shared_v4(b_st + d_im + d_k2, hm[4], hm[5], hm[6], hm[7]);
             st_shared_v4(b_st + d_im + d_lo, lm[0], lm[1], lm[2], lm[3]);
-            st_shared_v4(b_st + d_im + d_lo + 128, lm[4], lm[5], lm[6], lm[7]);
+            st_shared_v4(b_st + d_im + d_lo + d_k2, lm[4], lm[5], lm[6], lm[7]);
           }
           }  // b_rows
           // the phase table of stage st + kTcFacGroup (next group) into its
@@ -943,7 +1010,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         ptx::fence_proxy_async_smem();
         ptx::named_barrier(1, kTcProducers);
         if (s_end < nst && (s_end & (kTcDrain - 1)) == 0) {
-          tc_fold(p, B.acc_cols, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
+          tc_fold(p, accfull, tmem, gbase + next_drain, next_drain == 0, abort_flag);
           ++next_drain;
         }
       }
@@ -960,7 +1027,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         *rmax = 0;
       }
     }
-    if (U.n_groups > 0) tc_final(p, B.acc_cols, W, U, accfull, tmem, gbase + U.n_groups - 1, U.n_groups > 1, abort_flag);
+    if (U.n_groups > 0) tc_final(p, W, U, accfull, tmem, gbase + U.n_groups - 1, U.n_groups > 1, abort_flag);
     if (U.n_groups == 0 && tid < U.rows) {
       // no nodes in this split: its share of the tile is zero
       float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
@@ -984,7 +1051,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     for (int e = tid; e < B.n_entries; e += kTcThreads) atomicOr(B.entries[e].error, kErrTimeout);
   if (warp == 0) {
     ptx::tc_fence_after();
-    ptx::tmem_dealloc(tmem, 2 * B.acc_cols);
+    ptx::tmem_dealloc(tmem, kTcTmemCols);
   }
 }
 

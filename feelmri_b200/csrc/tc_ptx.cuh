@@ -115,6 +115,21 @@ __device__ inline uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
   return d;                // base offset 0, legacy LBO mode, layout SWIZZLE_NONE
 }
 
+// Shared-memory matrix descriptor of a K-major operand in the 64-byte
+// swizzled layout (rows of 64 bytes, 16-byte chunks XOR-permuted by address
+// bits 7-8, 8-row groups 512 bytes apart): start address (a tile start, or
+// plus 32 bytes for the second K step of 16 elements), LBO unused (encoded
+// 1), SBO 512, descriptor version 1, base offset 0, swizzle mode 64B (4).
+__device__ inline uint64_t smem_desc_sw64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;                  // LBO (ignored within one swizzle row)
+  d |= (uint64_t)(512 >> 4) << 32;         // SBO
+  d |= (uint64_t)1 << 46;                  // version
+  d |= (uint64_t)4 << 61;                  // SWIZZLE_64B
+  return d;
+}
+
 // Instruction descriptor of kind::f16 with BF16 A and B, FP32 accumulate,
 // both operands K-major, shape M x N.
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(uint32_t M, uint32_t N) {
@@ -132,6 +147,33 @@ __device__ inline void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
+}
+
+// The same MMA executed by a whole warp with only lane 0 issuing it (the
+// predicate is evaluated inside the instruction sequence, so the warp stays
+// converged and the warp-uniform descriptors need no per-thread moves).
+__device__ inline void mma_bf16_lane0(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                      uint32_t accumulate, uint32_t lane) {
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "setp.eq.u32 q, %5, 0;\n\t"
+      "@q tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(lane));
+  // no memory clobber: the MMA reads shared memory through the async proxy
+  // (ordered by the writers' proxy fence and the block barrier before it),
+  // and as a volatile asm it stays in order with the other volatile asm
+  // (waits, barriers, commits), so a clobber would only force the caller's
+  // values out of registers between consecutive MMAs
+}
+
+// mma_commit issued by lane 0 of a converged warp.
+__device__ inline void mma_commit_lane0(uint64_t *bar, uint32_t lane) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\t"
+      "setp.eq.u32 q, %1, 0;\n\t"
+      "@q tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}" ::"r"(smem_addr(bar)),
+      "r"(lane));
 }
 
 // Arrives on `bar` once all previously issued tcgen05.mma of this thread

@@ -117,3 +117,36 @@ def test_precision_config_reduced_nodes(cuda):
     assert K.shape == (*traj.shape, C)
     err = fp64.rel_l2(K.reshape(S, C)[pick], ref)
     assert err < 1e-4, err
+
+
+@pytest.mark.parametrize("precision,tol", [("f32", 1e-5), ("bf16x3", 2e-5)])
+def test_node_partition_sums_to_whole_mesh(cuda, precision, tol):
+    # the multi-GPU scheme (Phantom.py:194-239, MPIUtilities.py:13-26) through
+    # the product path: each part's local lumped mass and Signal, summed as
+    # gather_data does, equals the Signal of the whole mesh (parts run one
+    # after another on this GPU; no collective is involved)
+    from feelmri_b200.distributed import distribute_mesh
+    mesh = W.tube(30_000, 0.012, 0.1)
+    traj = W.cartesian(res=(16, 24, 8))
+    rng = np.random.default_rng(4)
+    N = mesh.n_nodes
+    Mxy = ((rng.normal(size=(N, 2)) + 1j * rng.normal(size=(N, 2))) * 0.1).astype(np.complex64)
+    phi = W.off_resonance(N, 20.0, 4)
+    _, T2 = W.tissue(N, 4)
+    vel = W.poiseuille_velocity(mesh.nodes, 0.012, v_max=1.0, period=60.0, n_frames=6)
+
+    def signal(elems, nodes, l2g):
+        w = _lumped(type(mesh)(nodes, elems), np.float32).astype(np.float32)
+        term = vel.terms[0]
+        from feelmri_b200.motion import SplineMotion, SplineTerm
+        local = SplineMotion([SplineTerm(term.kind, term.coeffs, term.knots, modes=term.modes[l2g],
+                                         period=term.period)])
+        return Signal(0, sp.diags(w).tocsc(), traj.points, traj.t, nodes.astype(np.float32), phi[l2g], T2[l2g],
+                      Mxy[l2g], local, precision=precision)
+
+    whole = signal(mesh.elems, mesh.nodes, np.arange(N))
+    total = np.zeros_like(whole)
+    for rank in range(3):
+        part = distribute_mesh(mesh.elems, mesh.nodes, 3, rank)
+        total += signal(part.elems, part.nodes, part.local_to_global)
+    assert fp64.rel_l2(total, whole) < tol
