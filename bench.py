@@ -195,7 +195,7 @@ def _max_over_ranks(dist, dev, value: float) -> float:
 
 
 def timed_steps(fn, steps: int, warmup: int, dev, local: int, ctx, kernels=("signal_tc", "signal_f32"),
-                dist=None, flush=None) -> dict:
+                dist=None, flush=None, nvtx: str = "step") -> dict:
     """W untimed steps, then K steps each bracketed by CUDA events on the
     launching stream, L2 flushed between them (outside the events), clocks
     sampled meanwhile, library kernel events on; barrier + synchronize on
@@ -214,12 +214,15 @@ def timed_steps(fn, steps: int, warmup: int, dev, local: int, ctx, kernels=("sig
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     with ClockSampler(local) as clk:
         torch.cuda.synchronize(dev)
+        # an NVTX range marks the timed steps for a profiler (no cost without one)
+        torch.cuda.nvtx.range_push(f"timed:{nvtx}")
         for a, b in ev:
             if flush is not None:
                 flush.zero_()
             a.record(stream)
             fn()
             b.record(stream)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize(dev)
     launches = _lib.launch_count() - l0
     _lib.timing(ctx, False)
@@ -332,10 +335,10 @@ def run_batching(args) -> dict | None:
 
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
     ctx = ops.ctx_for(dev)
-    tc = timed_steps(step_tc, args.steps, args.warmup, dev, local, ctx, dist=dist, flush=flush)
+    tc = timed_steps(step_tc, args.steps, args.warmup, dev, local, ctx, dist=dist, flush=flush, nvtx="bf16x3")
     batch.status()
     f32_steps = max(3, min(args.steps, args.f32_steps))
-    f32 = timed_steps(step_32, f32_steps, 2, dev, local, ctx, dist=dist, flush=flush)
+    f32 = timed_steps(step_32, f32_steps, 2, dev, local, ctx, dist=dist, flush=flush, nvtx="f32")
 
     # the same split-BF16 step captured once in a CUDA graph and replayed
     stream = torch.cuda.Stream(device=dev)
