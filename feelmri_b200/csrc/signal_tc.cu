@@ -24,7 +24,7 @@
 // Block (persistent, one per SM, 16 warps): in factored units warps 0-7
 // write the A tiles and warps 8-15 the B tiles and the phase tables; in
 // generic units every warp writes A (16 nodes per pipeline stage, a ring of
-// 4 stages in shared memory in the UMMA no-swizzle K-major layout).
+// 4 stages in shared memory in the 64-byte swizzled K-major layout).
 // Threads 0-127 also derive the node blocks.  After each group's
 // barrier one thread (warp 7, lane 0) issues the group's MMAs; warp 0 owns
 // the tensor memory.  tcgen05.commit frees a ring slot when the MMAs that
@@ -108,6 +108,7 @@ struct TcDev {
   int stacked;       // items hold several runs (D in the A rows, B without decay)
   int mm_ld;         // row stride of MM (float2): this group's columns, padded to even
   int tma;           // node blocks are staged by bulk copies (aligned inputs, room in smem)
+  int mstage;        // 3 r: a single POD term's mode rows are staged with each node block (0: read from global)
   const int *plan;  // device: [2] factored items, [3] generic items, [4] splits, [5] nodes per split
   float2 *partials; // (splits, S, V) when splits > 1
   float2 *out;
@@ -184,6 +185,10 @@ __host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
 __host__ __device__ inline uint32_t tc_raw_bytes(int mm_ld) {
   return kTcBlockNodes * (12 + 4 + 4 + 8 * mm_ld);
 }
+
+// Bytes of one node block's POD mode rows ([128][3 r] floats), staged after
+// the raw block when TcDev::mstage (= 3 r) is set.
+__host__ __device__ inline uint32_t tc_mode_bytes(int mstage) { return kTcBlockNodes * 4 * (uint32_t)mstage; }
 
 // Byte offset of element (row, k) of a K-major operand tile with 32 K
 // elements (64-byte rows) in the 64-byte swizzled layout: row r at r * 64,
@@ -346,7 +351,7 @@ __device__ inline void tc_load_raw(const TcDev &p, int64_t n, TcRaw &r) {
 // off-resonance rotated weights W' = (M Mxy)[n, v] exp(-t / T2) exp(i phi t).
 // Nodes past the range get position 0 and zero weights, so they add nothing.
 __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, const TcRaw &r, const float *wrun,
-                                 double *pos, float2 *wblk, int slot, int *rmax) {
+                                 double *pos, float2 *wblk, int slot, int *rmax, const float *smodes = nullptr) {
   if (n < U.n_end) {
     float x = r.x, y = r.y, z = r.z;
     const int rm = tc_reg_modes(p);
@@ -364,7 +369,22 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
       x = x + tx; y = y + ty; z = z + tz;
     } else if (p.md.kind == FM_MOTION_TERMS) {
       float dx, dy, dz;
-      motion_disp(p.md, wrun, n, p.N, dx, dy, dz);
+      if (smodes) {
+        // the single POD term's sum (motion_disp's products in its order),
+        // the mode row read from the staged block
+        const int rk = p.md.terms[0].n_modes;
+        const float *Phi = smodes + slot * 3 * rk, *wk = wrun + p.md.slot0[0];
+        dx = 0.f; dy = 0.f; dz = 0.f;
+#pragma unroll 1
+        for (int m = 0; m < rk; ++m) {
+          const float wm = wk[m];
+          dx = fmaf(Phi[m], wm, dx);
+          dy = fmaf(Phi[rk + m], wm, dy);
+          dz = fmaf(Phi[2 * rk + m], wm, dz);
+        }
+      } else {
+        motion_disp(p.md, wrun, n, p.N, dx, dy, dz);
+      }
       x = x + dx; y = y + dy; z = z + dz;
     } else if (p.table) {
       const float *d = p.table + ((int64_t)U.it.run * p.N + n) * 3;
@@ -416,6 +436,7 @@ __device__ inline void tc_derive(const TcDev &p, const TcUnit &U, int64_t n, con
 // copies into the staging area (thread 0; completion on rawfull), any other
 // block by register loads.  Otherwise the block is derived into the other
 // node buffer.  raw_seq counts the staged blocks (the rawfull phase).
+template <bool kModes>
 __device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, uint32_t blk, bool request,
                                       TcRaw &raw, uint32_t &raw_seq, unsigned char *staging, uint64_t *rawfull,
                                       const float *wrun, double *pos_next, float2 *w_next,
@@ -427,19 +448,25 @@ __device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, 
   float *sT2 = sr0 + 3 * kTcBlockNodes;
   float *sphi = sT2 + kTcBlockNodes;
   float2 *sMM = reinterpret_cast<float2 *>(sphi + kTcBlockNodes);
+  // the block's POD mode rows, after the raw block (TcDev::mstage)
+  float *smodes = reinterpret_cast<float *>(staging + tc_raw_bytes(p.mm_ld));
   if (request) {
     if (staged) {
       if (tid == 0) {
         // the staging area's previous readers (the last block's derive) are
         // past this stage's barriers; order their reads before the copies
         ptx::fence_proxy_async_smem();
-        ptx::mbar_arrive_expect_tx(rawfull, tc_raw_bytes(p.mm_ld));
+        ptx::mbar_arrive_expect_tx(rawfull, tc_raw_bytes(p.mm_ld) + (kModes ? tc_mode_bytes(p.mstage) : 0u));
         ptx::bulk_copy_g2s(sr0, p.r0 + 3 * n0, 12 * kTcBlockNodes, rawfull);
         ptx::bulk_copy_g2s(sT2, p.T2 + n0, 4 * kTcBlockNodes, rawfull);
         ptx::bulk_copy_g2s(sphi, p.phi + n0, 4 * kTcBlockNodes, rawfull);
         ptx::bulk_copy_g2s(sMM, p.MM + n0 * p.mm_ld, 8 * kTcBlockNodes * p.mm_ld, rawfull);
+        // mode rows of node n0 onwards: 12 r bytes per node, n0 a multiple of
+        // 16 and the rows 16-byte aligned (checked on the host)
+        if (kModes && p.mstage)
+          ptx::bulk_copy_g2s(smodes, p.md.terms[0].modes + n0 * p.mstage, tc_mode_bytes(p.mstage), rawfull);
       }
-      tc_prefetch_modes(p, n1, raw);
+      if (!(kModes && p.mstage)) tc_prefetch_modes(p, n1, raw);
     } else if (n1 < U.n_end) {
       tc_load_raw(p, n1, raw);
     }
@@ -456,7 +483,7 @@ __device__ inline void tc_stage_block(const TcDev &p, const TcUnit &U, int tid, 
       for (int v = 0; v < kTcVGroup; ++v)
         if (v < p.VG) raw.m[v] = sMM[tid * p.mm_ld + v];
     }
-    tc_derive(p, U, n1, raw, wrun, pos_next, w_next, tid, rmax);
+    tc_derive(p, U, n1, raw, wrun, pos_next, w_next, tid, rmax, kModes && staged && p.mstage ? smodes : nullptr);
   }
 }
 
@@ -638,6 +665,9 @@ __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, 
   if ((st % kTcDrain) == kTcDrain - 1 || st == n_stages - 1) ptx::mma_commit_lane0(accfull, lane);
 }
 
+// kModes: some entry stages POD mode rows with its node blocks (TcDev::mstage);
+// the instance without that code is the one every other launch uses.
+template <bool kModes>
 __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_constant__ TcBatchDev B) {
   extern __shared__ __align__(1024) unsigned char smem[];
   // work sizes come from the device-side plan, so the launch needs no host
@@ -813,7 +843,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
           const uint32_t g = g0 + st, s = g & (kTcStages - 1);
           const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
           if (loader && blk + 1 < n_blocks && (j == 4 || j == 6))
-            tc_stage_block(p, U, tid, blk, j == 4, raw, raw_seq, smem + L.raw, rawfull, wrun,
+            tc_stage_block<kModes>(p, U, tid, blk, j == 4, raw, raw_seq, smem + L.raw, rawfull, wrun,
                            pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
                            rmax);
           // the MMAs that last read stage s were sent at an earlier barrier
@@ -873,7 +903,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         // a group's stages lie in one node block (groups divide the blocks)
         const uint32_t jg = sg & (kTcStagesPerBlock - 1), blk = sg / kTcStagesPerBlock, buf = blk & 1;
         if (loader && blk + 1 < n_blocks && (jg == 2 || jg == 4))
-          tc_stage_block(p, U, tid, blk, jg == 2, raw, raw_seq, smem + L.raw, rawfull, wrun,
+          tc_stage_block<kModes>(p, U, tid, blk, jg == 2, raw, raw_seq, smem + L.raw, rawfull, wrun,
                          pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
                          rmax);
         tc_wait_group(empty, g0 + s_end - 1, abort_flag);
@@ -1498,6 +1528,14 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
       const bool aligned = ((uintptr_t)p.r0 % 16 == 0) && ((uintptr_t)p.T2 % 16 == 0) &&
                            ((uintptr_t)p.phi % 16 == 0) && ((uintptr_t)p.MM % 16 == 0);
       p.tma = aligned && tc_smem_layout(p.NT, p.wrows, p.Qt).total + tc_raw_bytes(p.mm_ld) <= kTcSmemMax;
+      // the mode rows of a single POD term of several modes are staged with
+      // the node blocks (a rank-1 term is held in registers instead) when
+      // they are 16-byte aligned and there is room after the raw block
+      if (p.tma && md.kind == FM_MOTION_TERMS && md.n_terms == 1 && md.terms[0].kind != FM_TERM_RESPIRATORY &&
+          md.terms[0].n_modes > kTcRegModes && (uintptr_t)md.terms[0].modes % 16 == 0 &&
+          tc_smem_layout(p.NT, p.wrows, p.Qt).total + tc_raw_bytes(p.mm_ld) +
+                  tc_mode_bytes(3 * md.terms[0].n_modes) <= kTcSmemMax)
+        p.mstage = 3 * md.terms[0].n_modes;
     }
   }
   tc_plan_kernel<<<1, 32, 0, st>>>(pl.plan, pl.n_groups, N, pl.max_splits, tune ? tune->split_nodes : 0);
@@ -1527,12 +1565,14 @@ static int tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc
   if (ne == 0) return FM_OK;
   int acc_cols = 32;
   size_t smem = 0;
+  bool modes = false;
   for (int e = 0; e < ne; ++e) {
+    modes = modes || host[e].mstage != 0;
     int NT = host[e].NT, ac = 32;
     while (ac < NT) ac <<= 1;
     if (ac > acc_cols) acc_cols = ac;
     const size_t sm = tc_smem_layout(NT, host[e].wrows, host[e].Qt).total +
-                      (host[e].tma ? tc_raw_bytes(host[e].mm_ld) : 0);
+                      (host[e].tma ? tc_raw_bytes(host[e].mm_ld) + tc_mode_bytes(host[e].mstage) : 0);
     if (sm > smem) smem = sm;
   }
   FM_REQUIRE(smem <= kTcSmemMax, FM_ERR_UNSUPPORTED, "%s: tile needs %zu bytes of shared memory", who, smem);
@@ -1554,8 +1594,9 @@ static int tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc
   B.acc_cols = acc_cols;
   {
     ScopedTimer timer(ctx, "signal_tc");
-    FM_CUDA(cudaFuncSetAttribute(signal_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    signal_tc_kernel<<<kSmCount, kTcThreads, smem, st>>>(B);
+    auto kernel = modes ? signal_tc_kernel<true> : signal_tc_kernel<false>;
+    FM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kernel<<<kSmCount, kTcThreads, smem, st>>>(B);
     count_launch();
     FM_TRY(check_launch("signal_tc_kernel"));
   }

@@ -186,3 +186,36 @@ def test_phase_range_is_checked(cuda, scale):
         # the context is still usable
         K = Signal(0, M, traj.points, traj.t, mesh.nodes.astype(np.float32), phi, T2, Mxy, None, precision="bf16x3")
         assert np.isfinite(K).all()
+
+
+def test_staged_mode_rows_match_global_reads(cuda):
+    """A POD term of several modes: the tensor-core form stages each node
+    block's mode rows in shared memory with the block's other inputs.  The
+    same call with the modes at an address that is not 16-byte aligned reads
+    them from global memory instead; both agree bit for bit, and with FP64."""
+    import torch
+    from feelmri_b200 import ops
+    from feelmri_b200._motion import lower
+    mesh, N, M, Mxy, phi, T2 = _case(n=6000, V=8, seed=3)
+    traj = W.radial3d(n_ro=16, n_spokes=96, kmax=500.0)
+    r0 = mesh.nodes.astype(np.float32)
+    pod = W.sinusoidal_pod(N, n_modes=10, amp=1e-3, period=50.0, n_frames=8, seed=4)
+    dev = torch.device("cuda", 0)
+    up = lambda a, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dt)
+    Mc = sp.csc_matrix(M)
+    inp = ops.SignalInputs(M=ops.SparseCSC(Mc.shape, up(Mc.indptr, torch.int32), up(Mc.indices, torch.int32),
+                                           up(Mc.data)),
+                           kx=up(traj.kx), ky=up(traj.ky), kz=up(traj.kz), t=up(traj.t), r0=up(r0), phi=up(phi),
+                           T2=up(T2), Mxy=up(Mxy, torch.complex64))
+    aligned = lower(pod, N, dev)
+    assert aligned.struct.terms[0].modes % 16 == 0 and aligned.struct.terms[0].n_modes == 10
+    K_staged = ops.signal(inp, aligned, "bf16x3").cpu().numpy()
+    shifted = lower(pod, N, dev)
+    rows = torch.empty(N * 30 + 1, dtype=torch.float32, device=dev)[1:]
+    rows.copy_(torch.from_numpy(np.ascontiguousarray(pod.terms[0].modes, np.float32).reshape(-1)).to(dev))
+    shifted.struct.terms[0].modes = rows.data_ptr()
+    shifted.keep.append(rows)
+    K_global = ops.signal(inp, shifted, "bf16x3").cpu().numpy()
+    np.testing.assert_array_equal(K_staged.view(np.uint64), K_global.view(np.uint64))
+    err = fp64.rel_l2(K_staged.reshape(*traj.shape, 8), _ref(M, traj, r0, phi, T2, Mxy, pod=pod))
+    assert err < TOL, err
