@@ -623,15 +623,18 @@ __device__ inline void tc_final(const TcDev &p, const TcWork &W, const TcUnit &U
 // n_stages stages): A_hi B_hi + A_hi B_lo + A_lo B_hi over the two K steps
 // into the accumulator (overwritten at a group's first stage); the stage's
 // shared memory is released by a commit to empty[s], and the group's
-// accumulator by a commit to accfull after the group's last stage.  Called by
+// accumulator by a commit to accfull after the group's last stage.  kFence:
+// the call orders its MMAs after the group barrier itself (otherwise the
+// caller has done so once for the group).  Called by
 // the whole issuing warp (warp 7): the descriptors are warp-uniform, and
 // lane 0 issues the MMAs and commits (it is the thread whose operations the
 // commits track).
+template <bool kFence>
 __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, uint32_t idesc, int NT,
                                 uint64_t *empty, uint64_t *accfull, uint32_t g, uint32_t st, uint32_t n_stages,
                                 uint32_t lane) {
   const uint32_t s = g % kTcStages;
-  ptx::tc_fence_after();
+  if (kFence) ptx::tc_fence_after();
   const uint32_t stage = sbase + L.stages + s * L.stage_bytes;
   // the drain group's first stage overwrites the accumulator; everything is
   // computed before the first MMA goes out
@@ -842,8 +845,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         for (uint32_t st = sg; st < s_end; ++st) {
           const uint32_t g = g0 + st, s = g & (kTcStages - 1);
           const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
-          if (loader && blk + 1 < n_blocks && (j == 4 || j == 6))
-            tc_stage_block<kModes>(p, U, tid, blk, j == 4, raw, raw_seq, smem + L.raw, rawfull, wrun,
+          if (loader && blk + 1 < n_blocks && (j == 0 || j == 4))
+            tc_stage_block<kModes>(p, U, tid, blk, j == 0, raw, raw_seq, smem + L.raw, rawfull, wrun,
                            pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
                            rmax);
           // the MMAs that last read stage s were sent at an earlier barrier
@@ -880,9 +883,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         ptx::fence_proxy_async_smem();
         // every writer of the group is done: its MMAs go out now
         ptx::named_barrier(1, kTcProducers);
-        if (warp == 7)
+        if (warp == 7) {
+          ptx::tc_fence_after();
           for (uint32_t st = sg; st < s_end; ++st)
-            tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst, lane);
+            tc_issue<false>(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst, lane);
+        }
         // an accumulation group ended with this group: fold it before the
         // next group's MMAs (which go out at the next barrier)
         if (s_end < nst && (s_end & (kTcDrain - 1)) == 0) {
@@ -960,7 +965,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         ptx::named_barrier(1, kTcProducers);
         if (warp == 7)
           for (uint32_t st = sg; st < s_end; ++st)
-            tc_issue(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst, lane);
+            tc_issue<true>(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst, lane);
         // an accumulation group ended with this group: fold it before the
         // next group's MMAs go out
         if (s_end < nst && (s_end & (kTcDrain - 1)) == 0) {
