@@ -76,14 +76,23 @@ def upload_many(items, device: torch.device) -> list:
         return _upload_many(items, device)
 
 
+_COPY_CHUNK = 8 << 20  # bytes of one staging copy task
+
+
 def _upload_many(items, device: torch.device) -> list:
     global _copy_pool
-    arrays, offs, total = [], [], 0
+    arrays, dtypes, offs, total = [], [], [], 0
     for a, dt in items:
-        arr = np.ascontiguousarray(np.asarray(a).astype(_NP_OF[dt], copy=False))
+        # the conversion to the device dtype happens in the staging copy
+        # (np.copyto rounds as astype does), on the copy threads
+        arr = np.asarray(a)
+        if not arr.flags.c_contiguous:
+            arr = np.ascontiguousarray(arr)
+        npdt = np.dtype(_NP_OF[dt])
         arrays.append(arr)
+        dtypes.append(npdt)
         offs.append(total)
-        total += (arr.nbytes + 255) & ~255
+        total += (arr.size * npdt.itemsize + 255) & ~255
     key = _index(device)
     st = _staging.get(key)
     if st is None or st[0].numel() < total:
@@ -93,29 +102,37 @@ def _upload_many(items, device: torch.device) -> list:
         ev.synchronize()  # the last transfer out of this buffer is done
     host = buf.numpy()
 
-    def put(i):
-        arr = arrays[i]
-        if arr.nbytes:
-            np.copyto(host[offs[i]:offs[i] + arr.nbytes].view(arr.dtype).reshape(arr.shape), arr)
-    big = [i for i, arr in enumerate(arrays) if arr.nbytes >= (1 << 20)]
-    for i, arr in enumerate(arrays):
-        if arr.nbytes < (1 << 20):
-            put(i)
-    if len(big) > 1:
+    # copy tasks: whole small arrays, large ones in chunks of elements
+    tasks = []
+    for i, (arr, npdt) in enumerate(zip(arrays, dtypes)):
+        n = arr.size
+        if n == 0:
+            continue
+        step = max(1, _COPY_CHUNK // npdt.itemsize)
+        for e0 in range(0, n, step):
+            tasks.append((i, e0, min(n, e0 + step)))
+
+    def put(task):
+        i, e0, e1 = task
+        arr, npdt = arrays[i], dtypes[i]
+        dst = host[offs[i]:offs[i] + arr.size * npdt.itemsize].view(npdt)
+        np.copyto(dst[e0:e1], arr.reshape(-1)[e0:e1], casting="unsafe")
+    if len(tasks) > 1 and total >= (2 << 20):
         if _copy_pool is None:
             from concurrent.futures import ThreadPoolExecutor
             _copy_pool = ThreadPoolExecutor(max_workers=8)
-        list(_copy_pool.map(put, big))
-    elif big:
-        put(big[0])
+        list(_copy_pool.map(put, tasks))
+    else:
+        for t in tasks:
+            put(t)
     dev_buf = torch.empty(max(total, 1), dtype=torch.uint8, device=device)
     dev_buf.copy_(buf[:max(total, 1)], non_blocking=True)
     ev = torch.cuda.Event()
     ev.record(torch.cuda.current_stream(device))
     _staging[key] = (buf, ev)
     out = []
-    for (a, dt), arr, o in zip(items, arrays, offs):
-        out.append(dev_buf[o:o + arr.nbytes].view(dt).reshape(arr.shape))
+    for (a, dt), arr, npdt, o in zip(items, arrays, dtypes, offs):
+        out.append(dev_buf[o:o + arr.size * npdt.itemsize].view(dt).reshape(arr.shape))
     return out
 
 

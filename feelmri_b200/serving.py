@@ -96,11 +96,31 @@ def footprint_bytes(req: Request) -> int:
     return int(state + traj + max(mass_setup, signal_ws) + (64 << 20))
 
 
+def _upload_items(req: Request) -> list:
+    """(host array, device dtype) of every input a Simulation uploads, in the
+    order Simulation unpacks them."""
+    t = req.traj
+    items = [(req.mesh.nodes, torch.float32), (req.T1, torch.float32), (req.T2, torch.float32),
+             (req.phi, torch.float32), (req.coils, torch.complex64), (t.kx, torch.float32),
+             (t.ky, torch.float32), (t.kz, torch.float32), (t.t, torch.float32)]
+    for b in req.blocks:
+        items += [(b.rf, torch.complex64), (b.G, torch.float32), (b.dt, torch.float32)]
+    if req.weights is not None:
+        items.append((req.weights, torch.float32))
+    return items
+
+
+PINNED_KSPACE_MAX = 64 << 20  # bytes of a request's k-space frames kept in pinned memory
+
+
 class Simulation:
     """Device-resident state of one request.  Construction queues the upload
-    and the mass assembly on `stream` and records `ready` there."""
+    and the mass assembly on `stream` and records `ready` there.  `uploaded`:
+    the request's inputs already on the device (in _upload_items order), when
+    several requests were sent up together."""
 
-    def __init__(self, req: Request, device: torch.device, stream: torch.cuda.Stream | None = None):
+    def __init__(self, req: Request, device: torch.device, stream: torch.cuda.Stream | None = None,
+                 uploaded: list | None = None):
         from .Assemble import mass_lumped
         from .FiniteElements import FiniteElement, QuadratureRule
         self.req = req
@@ -109,14 +129,7 @@ class Simulation:
         self.frame = 0
         N, t = req.n_nodes, req.traj
         with torch.cuda.stream(self.stream):
-            items = [(req.mesh.nodes, torch.float32), (req.T1, torch.float32), (req.T2, torch.float32),
-                     (req.phi, torch.float32), (req.coils, torch.complex64), (t.kx, torch.float32),
-                     (t.ky, torch.float32), (t.kz, torch.float32), (t.t, torch.float32)]
-            for b in req.blocks:
-                items += [(b.rf, torch.complex64), (b.G, torch.float32), (b.dt, torch.float32)]
-            if req.weights is not None:
-                items.append((req.weights, torch.float32))
-            dev = ops.upload_many(items, device)
+            dev = uploaded if uploaded is not None else ops.upload_many(_upload_items(req), device)
             self.r0, self.T1, self.T2, self.phi, self.coils, kx, ky, kz, tt = dev[:9]
             self.blocks = [(dev[9 + 3 * i], dev[10 + 3 * i], dev[11 + 3 * i], b.t0, b.empty)
                            for i, b in enumerate(req.blocks)]
@@ -138,7 +151,15 @@ class Simulation:
                                         Mxy=self.cols)
             self.ready = torch.cuda.Event()
             self.ready.record(self.stream)
-        self.kspace = np.empty((req.frames, *t.shape, req.n_coils), np.complex64)
+        # k-space frames land in pinned memory straight from the device when
+        # they are small enough (no second host copy), else via staging
+        shape = (req.frames, *t.shape, req.n_coils)
+        if int(np.prod(shape)) * 8 <= PINNED_KSPACE_MAX:
+            self._kspace_t = torch.empty(shape, dtype=torch.complex64, pin_memory=True)
+            self.kspace = self._kspace_t.numpy()
+        else:
+            self._kspace_t = None
+            self.kspace = np.empty(shape, np.complex64)
 
     @property
     def done(self) -> bool:
@@ -204,9 +225,13 @@ def launch_iteration(sims: list[Simulation], tuning: ops.Tuning = SERVING_TUNING
         sb.enqueue()
     host = []
     for s in sims:
-        h = torch.empty(s.out.shape, dtype=torch.complex64, pin_memory=True)
-        h.copy_(s.out, non_blocking=True)
-        host.append(h)
+        if s._kspace_t is not None:
+            s._kspace_t[s.frame].copy_(s.out, non_blocking=True)
+            host.append(None)
+        else:
+            h = torch.empty(s.out.shape, dtype=torch.complex64, pin_memory=True)
+            h.copy_(s.out, non_blocking=True)
+            host.append(h)
     return Iteration(sims, sb, host, stream, keep)
 
 
@@ -217,7 +242,8 @@ def finish_iteration(it: Iteration) -> None:
         it.batch.status()
     it.stream.synchronize()
     for s, h in zip(it.sims, it.host):
-        s.kspace[s.frame] = h.numpy()
+        if h is not None:
+            s.kspace[s.frame] = h.numpy()
         s.frame += 1
 
 
@@ -235,7 +261,19 @@ def simulate_batch(requests: list[Request], device: torch.device | None = None,
     k-spaces come back through pinned memory.  Returns one (n_ro, n_lines,
     n_kz, C) complex64 array per request."""
     device = device or ops.require_cuda()
-    sims = [Simulation(r, device, torch.cuda.current_stream(device)) for r in requests]
+    stream = torch.cuda.current_stream(device)
+    # every request's inputs in one staging pass (copies on several threads)
+    # and one host-to-device transfer
+    items, counts = [], []
+    for r in requests:
+        it = _upload_items(r)
+        items += it
+        counts.append(len(it))
+    dev = ops.upload_many(items, device) if items else []
+    sims, k = [], 0
+    for r, c in zip(requests, counts):
+        sims.append(Simulation(r, device, stream, uploaded=dev[k:k + c]))
+        k += c
     run_iteration(sims, tuning or SERVING_TUNING)
     return [s.kspace[0] for s in sims]
 
