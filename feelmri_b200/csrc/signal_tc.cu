@@ -79,15 +79,17 @@ constexpr uint32_t kAStageBytes = kTcRows * 2 * kTcNodes * 2;  // 128 rows x 32 
 struct TcRun {
   int start, P, Q, factored;
 };
-// A work item: rows p0.. and columns q0.. of run `run`, or (nrun > 1) the
-// whole slabs of runs run .. run + nrun - 1 stacked along the rows: row
-// r P + p is line p of run `run + r`, and every run shares the columns.
-// The runs then differ only in their times, so each run's decay and
-// off-resonance factor D_r(n) = exp(-t_r / T2_n) exp(i phi_n t_r) moves into
-// its A rows (A = exp(-2 pi i kp . r) D_r) and B = exp(-2 pi i kq . r) (M Mxy)
-// is the same for all of them: the whole product is read.
+// A work item: `rows` lines from line p0 and columns q0.. of run `run`, or
+// (stacked problems) `rows` consecutive lines of the problem's runs laid end
+// to end, from line p0 of run `run` on: unit row i is line (p0 + i) % P of
+// run run + (p0 + i) / P (P lines per run), nrun runs in all, and every run
+// shares the columns.  The runs then differ only in their times, so each
+// run's decay and off-resonance factor D_r(n) = exp(-t_r / T2_n)
+// exp(i phi_n t_r) moves into its A rows (A = exp(-2 pi i kp . r) D_r) and
+// B = exp(-2 pi i kq . r) (M Mxy) is the same for all of them: the whole
+// product is read.
 struct TcItem {
-  int run, p0, q0, nrun;
+  int run, p0, q0, nrun, rows;
 };
 
 struct TcDev {
@@ -240,7 +242,7 @@ struct TcUnit {
   TcItem it;
   TcRun run;  // the first run
   int split, P_tile, Q_tile, n_stages, n_groups;
-  int rows, pairs;  // active A rows (nrun P_tile) and column pairs (Q_tile VG)
+  int rows, pairs;  // active A rows and column pairs (Q_tile VG); P_tile: lines per run when stacked
   int64_t n_begin, n_end;
 };
 
@@ -250,15 +252,27 @@ __device__ inline TcUnit tc_unit(const TcDev &p, const TcWork &W, int u) {
   U.split = u / W.n_items;
   U.it = p.items[W.item0 + item];
   U.run = p.runs[U.it.run];
-  U.P_tile = min(kTcRows, U.run.P - U.it.p0);
+  U.P_tile = p.stacked ? U.run.P : min(kTcRows, U.run.P - U.it.p0);
   U.Q_tile = min(p.Qt, U.run.Q - U.it.q0);
-  U.rows = U.it.nrun * U.P_tile;
+  U.rows = U.it.rows;
   U.pairs = U.Q_tile * p.VG;
   U.n_begin = (int64_t)U.split * W.chunk;
   U.n_end = min(p.N, U.n_begin + W.chunk);
   U.n_stages = U.n_end > U.n_begin ? (int)ceil_div(U.n_end - U.n_begin, kTcNodes) : 0;
   U.n_groups = (int)ceil_div(U.n_stages, kTcDrain);
   return U;
+}
+
+// Run (relative to the unit's first) and line of unit row `row` (TcItem).
+__device__ inline void tc_row_line(const TcDev &p, const TcUnit &U, int row, int &r, int &line) {
+  if (p.stacked) {
+    const int lr = U.it.p0 + row;
+    r = lr / U.P_tile;
+    line = lr % U.P_tile;
+  } else {
+    r = 0;
+    line = U.it.p0 + row;
+  }
 }
 
 // Bounded wait that gives up at once after any earlier timeout of the block
@@ -568,11 +582,12 @@ __device__ inline void tc_final(const TcDev &p, const TcWork &W, const TcUnit &U
   const int NH = p.NT >> 1;
   const bool row_ok = row < U.rows;
   float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
-  // row r P_tile + pl is line pl of run `run + r`; every run shares the column pairs
-  const int r_row = row_ok ? row / U.P_tile : 0, pl = row_ok ? row % U.P_tile : 0;
+  // every run of a stacked unit shares the column pairs
+  int r_row = 0, line = 0;
+  if (row_ok) tc_row_line(p, U, row, r_row, line);
   const int qvg = U.Q_tile * p.VG;
   const int start = row_ok ? p.runs[U.it.run + r_row].start : 0;
-  const int s_row = start + (U.run.factored ? (U.it.p0 + pl) * p.n_kz + U.it.q0 : U.it.p0 + pl);
+  const int s_row = start + (U.run.factored ? line * p.n_kz + U.it.q0 : line);
   const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
   const int n_acc = tc_parts(p.NT), AW = p.NT, sum_col = tc_sum_col(p.NT);
   for (int c0 = (warp >> 2) * 8; c0 < NH; c0 += 32) {
@@ -760,11 +775,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     int a_drow = 0;      // A of a stacked unit: the row's D row in the node buffer
     if (a_role) {
       if (row < U.rows) {
-        // row r P_tile + pl belongs to run `run + r` (r = 0 unless stacked)
-        const int r = row / U.P_tile, pl = row % U.P_tile;
+        // the row's run (r = 0 unless stacked) and line
+        int r, line;
+        tc_row_line(p, U, row, r, line);
         a_drow = VG + r;
         const int start = r == 0 ? U.run.start : p.runs[U.it.run + r].start;
-        const int s_p = start + (fac ? (U.it.p0 + pl) * p.n_kz : U.it.p0 + pl);
+        const int s_p = start + (fac ? line * p.n_kz : line);
         kx0 = p.kx[s_p];
         ky0 = p.ky[s_p];
         kz0 = p.kz[s_p];
@@ -1066,9 +1082,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     if (U.n_groups == 0 && tid < U.rows) {
       // no nodes in this split: its share of the tile is zero
       float2 *dst = W.out + (int64_t)U.split * p.S * p.V;
-      const int r = tid / U.P_tile, pl = tid % U.P_tile;
+      int r, line;
+      tc_row_line(p, U, tid, r, line);
       const int start = p.runs[U.it.run + r].start;
-      const int s_row = start + (fac ? (U.it.p0 + pl) * p.n_kz + U.it.q0 : U.it.p0 + pl);
+      const int s_row = start + (fac ? line * p.n_kz + U.it.q0 : line);
       for (int q = 0; q < U.Q_tile; ++q)
         for (int v = 0; v < VG; ++v) dst[(int64_t)(s_row + q) * p.V + p.v0 + v] = make_float2(0.f, 0.f);
     }
@@ -1157,11 +1174,13 @@ __global__ void tc_stack_check_kernel(const float *__restrict__ kx, const float 
 }
 
 // Item counts per run, factored runs in one list and the rest in another.
-// With stacking (stack != nullptr and *stack set), every R-th run opens one
-// item of up to R runs.
+// With stacking (stack != nullptr and *stack set) the runs' P lines are laid
+// end to end and cut into items of RU lines: run g opens the items whose
+// first line falls in it.
+__device__ inline int64_t tc_packed_first(int64_t g, int P, int RU) { return ceil_div(g * P, (int64_t)RU); }
 __global__ void tc_count_kernel(const TcRun *__restrict__ runs, const int *__restrict__ counts, int Qt,
                                 int *__restrict__ nf, int *__restrict__ ng, int64_t S, const int *__restrict__ stack,
-                                int R) {
+                                int P, int RU) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = counts[0];
   if (g > S) return;
@@ -1170,8 +1189,8 @@ __global__ void tc_count_kernel(const TcRun *__restrict__ runs, const int *__res
     ng[g] = 0;
     return;
   }
-  if (stack && *stack && R > 1) {
-    nf[g] = (g % R == 0) ? 1 : 0;
+  if (stack && *stack) {
+    nf[g] = (int)(tc_packed_first(g + 1, P, RU) - tc_packed_first(g, P, RU));
     ng[g] = 0;
     return;
   }
@@ -1185,7 +1204,7 @@ __global__ void tc_count_kernel(const TcRun *__restrict__ runs, const int *__res
 // go to plan[2] and plan[3].
 __global__ void tc_fill_kernel(const TcRun *__restrict__ runs, const int *__restrict__ counts, int Qt,
                                const int *__restrict__ of, const int *__restrict__ og, TcItem *__restrict__ items,
-                               int *__restrict__ plan, const int *__restrict__ stack, int R) {
+                               int *__restrict__ plan, const int *__restrict__ stack, int P, int RU) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = counts[0];
   if (g > n) return;
@@ -1194,14 +1213,18 @@ __global__ void tc_fill_kernel(const TcRun *__restrict__ runs, const int *__rest
     plan[3] = og[n];
     return;
   }
-  if (stack && *stack && R > 1) {
-    if (g % R == 0) {
+  if (stack && *stack) {
+    const int64_t i0 = tc_packed_first(g, P, RU), i1 = tc_packed_first(g + 1, P, RU);
+    const int64_t total = (int64_t)n * P;
+    for (int64_t i = i0; i < i1; ++i) {
+      const int64_t L0 = i * RU;
       TcItem t;
       t.run = g;
-      t.p0 = 0;
+      t.p0 = (int)(L0 - (int64_t)g * P);
       t.q0 = 0;
-      t.nrun = (n - g) < R ? (n - g) : R;
-      items[of[g]] = t;
+      t.rows = (int)((total - L0) < RU ? (total - L0) : RU);
+      t.nrun = (int)((L0 + t.rows - 1) / P - g + 1);
+      items[of[g] + (i - i0)] = t;
     }
     return;
   }
@@ -1218,6 +1241,7 @@ __global__ void tc_fill_kernel(const TcRun *__restrict__ runs, const int *__rest
       t.p0 = a * kTcRows;
       t.q0 = b * qt;
       t.nrun = 1;
+      t.rows = (r.P - t.p0) < kTcRows ? (r.P - t.p0) : kTcRows;
       items[base + a * nq + b] = t;
     }
 }
@@ -1397,21 +1421,35 @@ static int tc_qt(const fm_signal_args *a, int VG, const fm_tc_tuning *tune) {
   }
 }
 
-// Runs per stacked unit for a column group: whole slabs only (lines <= 128
-// rows, kz within one tile), at most 128 rows (kTcMaxStack runs), and only
-// without motion (the runs then share node positions).  The node buffers
-// hold the VG weight rows and one D row per run.
+// Runs a stacked unit may touch, for a column group: stacking needs whole
+// kz slabs within one tile and no motion (the runs then share node
+// positions).  Units take 128 consecutive lines of the runs laid end to end,
+// so a unit touches 128 / P runs when P divides 128, else up to
+// ceil(127 / P) + 1; at most kTcMaxStack, and fewer when the node buffers (VG
+// weight rows and one D row per run) would not fit in shared memory.
 constexpr int kTcMaxStack = 16;
 static int tc_stack_runs(const fm_signal_args *a, int VG, int Qt) {
   if (a->motion && a->motion->kind != FM_MOTION_NONE) return 1;
-  if (a->n_kz < 2 || a->n_lines * a->n_kz < 2 || a->n_kz > Qt || a->n_lines > kTcRows) return 1;
-  int R = kTcRows / (int)a->n_lines;
+  if (a->n_kz < 2 || a->n_lines * a->n_kz < 2 || a->n_kz > Qt) return 1;
+  const int P = (int)a->n_lines;
+  int R = P >= kTcRows ? 2 : (kTcRows % P == 0 ? kTcRows / P : (kTcRows - 1 + P - 1) / P + 1);
   if (R > kTcMaxStack) R = kTcMaxStack;
   // the tiles and node buffers must fit in shared memory
   int NT, acc;
   tc_shape(Qt, VG, NT, acc);
   while (R > 1 && tc_smem_layout(NT, VG + R, Qt).total > kTcSmemMax) --R;
   return R < 2 ? 1 : R;
+}
+
+// Lines per stacked unit (RU) for P lines per run and units touching at most
+// R runs: all 128 rows when that keeps within R runs, else whole runs
+// (R P lines, units then start at run boundaries) or (R - 1) P lines (a unit
+// starting inside a run then still touches at most R runs).
+static int tc_pack_rows(int P, int R) {
+  if ((int64_t)R * P <= kTcRows) return R * P;
+  if (kTcRows % P == 0) return kTcRows;
+  if ((kTcRows - 1 + P - 1) / P + 1 <= R) return kTcRows;
+  return (R - 1) * P;
 }
 
 static void tc_shape(int Qt, int VG, int &NT, int &acc_cols) {
@@ -1482,11 +1520,12 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
     const int VG = (int)((V - v0) < kTcVGroup ? (V - v0) : kTcVGroup);
     const int Qt_f = tc_qt(a, VG, tune);
     const int R = tc_stack_runs(a, VG, Qt_f);
+    const int RU = R > 1 ? tc_pack_rows((int)a->n_lines, R) : 0;
     const int *stack = R > 1 ? pl.stack : nullptr;
     TcItem *items = pl.items + (size_t)g * (2 * S + 2);
     int *plan = pl.plan + 8 * g;
     const unsigned gb = (unsigned)ceil_div(S + 1, 256);
-    tc_count_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.nf, pl.ng, S, stack, R);
+    tc_count_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.nf, pl.ng, S, stack, (int)a->n_lines, RU);
     count_launch();
     FM_TRY(check_launch("tc_count_kernel"));
     size_t cb = pl.runs.cub_bytes;
@@ -1494,7 +1533,8 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
     cb = pl.runs.cub_bytes;
     FM_CUDA(cub::DeviceScan::ExclusiveSum(pl.runs.cub_tmp, cb, pl.ng, pl.og, (int)(S + 1), st));
     count_launch(2);
-    tc_fill_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.of, pl.og, items, plan, stack, R);
+    tc_fill_kernel<<<gb, 256, 0, st>>>(pl.tcruns, pl.runs.counts, Qt_f, pl.of, pl.og, items, plan, stack,
+                                       (int)a->n_lines, RU);
     count_launch();
     FM_TRY(check_launch("tc_fill_kernel"));
     for (int kind = 0; kind < 2; ++kind) {

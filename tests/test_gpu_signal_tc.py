@@ -154,6 +154,23 @@ def test_stacked_small_slabs(cuda):
     assert fp64.rel_l2(K, K32) < TOL
 
 
+@pytest.mark.parametrize("n_lines", [77, 140])
+def test_stacked_lines_across_runs(cuda, n_lines):
+    # slabs whose line count does not divide the 128 rows of a unit (77) or
+    # exceeds them (140): units take 128 consecutive lines of the runs laid
+    # end to end, so a unit starts inside one run and ends inside another;
+    # every sample must come out once, with its own run's decay
+    mesh, N, M, Mxy, phi, T2 = _case(n=3000, V=2, seed=8)
+    traj = W.cartesian(res=(7, n_lines, 8))
+    r0 = mesh.nodes.astype(np.float32)
+    K = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None, precision="bf16x3")
+    idx = np.random.default_rng(9).choice(traj.n_samples, 1500, replace=False)
+    err = fp64.rel_l2(K.reshape(traj.n_samples, -1)[idx], _ref(M, traj, r0, phi, T2, Mxy, idx=idx))
+    assert err < TOL, err
+    K32 = Signal(0, M, traj.points, traj.t, r0, phi, T2, Mxy, None)
+    assert fp64.rel_l2(K, K32) < TOL
+
+
 def test_unstackable_runs_fall_back(cuda):
     # kz offsets that change from run to run: the stacking check must refuse
     mesh, N, M, Mxy, phi, T2 = _case(n=3000, V=1, seed=6)
