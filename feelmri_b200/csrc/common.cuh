@@ -23,6 +23,11 @@ struct fm_ctx {
   bool timing = false;
   std::vector<fm_timed_launch> timed;
   std::vector<cudaEvent_t> event_pool;
+  // helper streams for independent per-problem work forked from `stream` and
+  // joined back into it (created on first use), with the fork event and one
+  // join event per helper
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_ev;
 };
 
 namespace fm {
@@ -36,6 +41,15 @@ inline void count_launch(int n = 1) { g_launches.fetch_add(n, std::memory_order_
 
 // Returns FM_ERR_CUDA with a message when the last launch failed.
 int check_launch(const char *what);
+
+// Makes sure ctx has at least k helper streams (and their events).
+int ctx_side_streams(fm_ctx *ctx, int k);
+// Work queued on ctx->stream so far comes before anything queued on the
+// first k helper streams after this call.
+int ctx_fork(fm_ctx *ctx, int k);
+// Everything queued on the first k helper streams comes before anything
+// queued on ctx->stream after this call.
+int ctx_join(fm_ctx *ctx, int k);
 
 #define FM_TRY(expr)                 \
   do {                               \

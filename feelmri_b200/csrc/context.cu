@@ -57,6 +57,44 @@ void timer_stop(fm_ctx *ctx, int slot) {
   cudaEventRecord(ctx->timed[slot].stop, ctx->stream);
 }
 
+int ctx_side_streams(fm_ctx *ctx, int k) {
+  if ((int)ctx->side.size() >= k) return FM_OK;
+  DeviceGuard g(ctx->device);
+  FM_REQUIRE(g.ok, FM_ERR_CUDA, "cudaSetDevice(%d) failed", ctx->device);
+  if (ctx->side_ev.empty()) {
+    cudaEvent_t e = nullptr;
+    FM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->side_ev.push_back(e);  // the fork event
+  }
+  while ((int)ctx->side.size() < k) {
+    cudaStream_t s = nullptr;
+    FM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      cudaStreamDestroy(s);
+      set_error(FM_ERR_CUDA, "cudaEventCreateWithFlags failed");
+      return FM_ERR_CUDA;
+    }
+    ctx->side.push_back(s);
+    ctx->side_ev.push_back(e);  // its join event
+  }
+  return FM_OK;
+}
+
+int ctx_fork(fm_ctx *ctx, int k) {
+  FM_CUDA(cudaEventRecord(ctx->side_ev[0], ctx->stream));
+  for (int i = 0; i < k; ++i) FM_CUDA(cudaStreamWaitEvent(ctx->side[i], ctx->side_ev[0], 0));
+  return FM_OK;
+}
+
+int ctx_join(fm_ctx *ctx, int k) {
+  for (int i = 0; i < k; ++i) {
+    FM_CUDA(cudaEventRecord(ctx->side_ev[1 + i], ctx->side[i]));
+    FM_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[1 + i], 0));
+  }
+  return FM_OK;
+}
+
 }  // namespace fm
 
 extern "C" {
@@ -134,6 +172,11 @@ int fm_ctx_destroy(fm_ctx *ctx) {
   FM_TRY(fm::ctx_ok(ctx));
   fm_ctx_timing_reset(ctx);
   for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+  {
+    fm::DeviceGuard g(ctx->device);
+    for (cudaEvent_t e : ctx->side_ev) cudaEventDestroy(e);
+    for (cudaStream_t s : ctx->side) cudaStreamDestroy(s);
+  }
   delete ctx;
   return FM_OK;
 }

@@ -1591,6 +1591,8 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
 
 // Signal for n problems: per-problem preparation, then one persistent
 // tensor-core launch over all of their work units, then the split sums.
+constexpr int kTcSideStreams = 4;  // helper streams for the per-problem preparations of a batch
+
 static int tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc_tuning *tune, void *ws,
                     size_t ws_bytes, const char *who) {
   cudaStream_t st = ctx->stream;
@@ -1602,11 +1604,22 @@ static int tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc
   FM_TRY(carve_ok(cv, who));
   std::vector<TcDev> host(tc_n_entries(probs, n) + 1);
   int ne = 0;
-  for (int i = 0; i < n; ++i) {
-    const int k = tc_prepare(&probs[i], plans[i], tune, host.data() + ne, st, who);
-    if (k < 0) return k;
-    ne += k;
+  // the problems' preparations are independent: with several problems they
+  // run on helper streams forked from the launch stream and joined back
+  // before the persistent launch (in a captured graph: parallel branches)
+  const int K = n >= 4 ? kTcSideStreams : 0;
+  if (K > 0) {
+    FM_TRY(ctx_side_streams(ctx, K));
+    FM_TRY(ctx_fork(ctx, K));
   }
+  int prep = FM_OK;
+  for (int i = 0; i < n && prep == FM_OK; ++i) {
+    const int k = tc_prepare(&probs[i], plans[i], tune, host.data() + ne, K > 0 ? ctx->side[i % K] : st, who);
+    if (k < 0) prep = k;
+    else ne += k;
+  }
+  if (K > 0) FM_TRY(ctx_join(ctx, K));
+  if (prep != FM_OK) return prep;
   if (ne == 0) return FM_OK;
   int acc_cols = 32;
   size_t smem = 0;
