@@ -206,13 +206,15 @@ def timed_steps(fn, steps: int, warmup: int, dev, local: int, ctx, kernels=("sig
     import torch
     from feelmri_b200 import _lib
     stream = torch.cuda.current_stream(dev)
+    ctxs = list(ctx) if isinstance(ctx, (list, tuple)) else [ctx]
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
-    _lib.timing_reset(ctx)
-    _lib.timing(ctx, True)
+    for c in ctxs:
+        _lib.timing_reset(c)
+        _lib.timing(c, True)
     l0 = _lib.launch_count()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     with ClockSampler(local) as clk:
@@ -228,19 +230,25 @@ def timed_steps(fn, steps: int, warmup: int, dev, local: int, ctx, kernels=("sig
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize(dev)
     launches = _lib.launch_count() - l0
-    _lib.timing(ctx, False)
+    for c in ctxs:
+        _lib.timing(c, False)
     if dist:
         dist.barrier()
     ms = [a.elapsed_time(b) for a, b in ev]
     total = _max_over_ranks(dist, dev, float(sum(ms)))
     out = {"ms_per_step": total / steps, "median_ms": statistics.median(ms), "total_ms": total,
            "steps": steps, "warmup": warmup, "launches": launches, "clocks": clk.summary()}
+    def query(name):
+        # summed over the contexts (the launch stream's and its helper streams')
+        ms_n = [_lib.timing_query(c, name) for c in ctxs]
+        return sum(m for m, _ in ms_n), sum(n for _, n in ms_n)
     for k in kernels:
-        k_ms, k_n = _lib.timing_query(ctx, k)
+        k_ms, k_n = query(k)
         if k_n:
             out[f"{k}_ms_per_launch"] = k_ms / k_n
             out[f"{k}_launches"] = k_n
-    b_ms, b_n = _lib.timing_query(ctx, "bloch")
+    b_ms, b_n = query("bloch")
+    # device time of the Bloch sweeps, summed over streams (they may overlap)
     out["bloch_ms_per_step"] = b_ms / steps
     return out
 
@@ -299,7 +307,7 @@ def _fp64_check(req, cols: np.ndarray, outs: dict, n_samples: int, seed: int) ->
 def run_batching(args) -> dict | None:
     import torch
     from feelmri_b200 import _lib, autotune, ops
-    from feelmri_b200.serving import Simulation
+    from feelmri_b200.serving import Simulation, enqueue_bloch_all, helper_streams
     rank, world, local, dev, dist = _dist()
     t0 = time.perf_counter()
     reqs = build_batch_requests(args.phantoms, seed=4 + 1000 * rank)
@@ -312,9 +320,10 @@ def run_batching(args) -> dict | None:
     problems = [(s.sig, m, s.out) for s, m in zip(sims, motions)]
     out32 = [torch.empty_like(s.out) for s in sims]
 
+    zero_frames = [0] * len(sims)
+
     def bloch_all():
-        for s in sims:
-            s.enqueue_bloch(0)
+        enqueue_bloch_all(sims, zero_frames)
 
     bloch_all()
     torch.cuda.synchronize(dev)
@@ -337,7 +346,10 @@ def run_batching(args) -> dict | None:
             ops.signal(s.sig, m, "f32", out=o, sync=False)
 
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
-    ctx = ops.ctx_for(dev)
+    ctx = [ops.ctx_for(dev)]
+    for st in helper_streams(dev):
+        with torch.cuda.stream(st):
+            ctx.append(ops.ctx_for(dev))
     tc = timed_steps(step_tc, args.steps, args.warmup, dev, local, ctx, dist=dist, flush=flush, nvtx="bf16x3")
     batch.status()
     f32_steps = max(3, min(args.steps, args.f32_steps))

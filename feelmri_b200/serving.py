@@ -192,6 +192,48 @@ class Simulation:
         return lower(self.req.pod, self.req.n_nodes, self.device)
 
 
+BLOCH_STREAMS = 4  # helper streams over which a set of simulations' Bloch blocks is spread
+_side_streams: dict = {}
+
+
+def helper_streams(device: torch.device, k: int = BLOCH_STREAMS) -> list:
+    """k helper streams of `device`, created once and reused."""
+    key = (device.index if device.index is not None else torch.cuda.current_device(), k)
+    ss = _side_streams.get(key)
+    if ss is None:
+        ss = [torch.cuda.Stream(device=device) for _ in range(k)]
+        _side_streams[key] = ss
+    return ss
+
+
+def enqueue_bloch_all(sims: list, frames: list | None = None) -> None:
+    """Every simulation's Bloch blocks (frame frames[i], else its current
+    frame) and coil columns.  The simulations are independent, so they are
+    spread over helper streams forked from the current stream and joined back
+    into it: small phantoms' sweeps run side by side instead of one after the
+    other (in a captured graph: parallel branches)."""
+    if not sims:
+        return
+    main = torch.cuda.current_stream(sims[0].device)
+    k = min(BLOCH_STREAMS, len(sims))
+    if k < 2:
+        for i, s in enumerate(sims):
+            s.enqueue_bloch(frames[i] if frames is not None else s.frame)
+        return
+    side = helper_streams(sims[0].device)[:k]
+    fork = torch.cuda.Event()
+    fork.record(main)
+    for st in side:
+        st.wait_event(fork)
+    for i, s in enumerate(sims):
+        with torch.cuda.stream(side[i % k]):
+            s.enqueue_bloch(frames[i] if frames is not None else s.frame)
+    for st in side:
+        join = torch.cuda.Event()
+        join.record(st)
+        main.wait_event(join)
+
+
 @dataclass
 class Iteration:
     """One frame of a set of simulations, queued on a stream."""
@@ -210,8 +252,7 @@ def launch_iteration(sims: list[Simulation], tuning: ops.Tuning = SERVING_TUNING
     stream = torch.cuda.current_stream(sims[0].device)
     for s in sims:
         stream.wait_event(s.ready)
-    for s in sims:
-        s.enqueue_bloch(s.frame)
+    enqueue_bloch_all(sims)
     batch, keep = [], []
     for s in sims:
         mo = s.motion(s.frame)
