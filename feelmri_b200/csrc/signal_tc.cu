@@ -46,6 +46,12 @@ namespace fm {
 constexpr int kTcRows = 128;        // UMMA M
 constexpr int kTcNodes = 16;        // nodes per stage -> K = 32 (two UMMA K steps)
 constexpr int kTcStages = 4;
+// Generic units use a ring of their own (kTcRingGen slots of their small
+// stages, which always fit), with their own barriers and stage counter, so
+// that a group's producers need not wait for the previous group's MMAs.  At
+// a unit's end every MMA has completed, so the two rings may share the
+// shared memory.
+constexpr int kTcRingGen = 8;
 constexpr int kTcBlockNodes = 128;  // nodes whose per-run data is formed together
 constexpr int kTcStagesPerBlock = kTcBlockNodes / kTcNodes;
 constexpr int kTcProducerWarps = 16;
@@ -69,7 +75,8 @@ constexpr int kTcGenGroup = 4;
 constexpr int kTcFacGroup = 2;
 constexpr int kTcEBufs = 2 * kTcFacGroup;
 constexpr uint64_t kTcWaitNs = 2000000000ull;
-static_assert(kTcGenGroup <= kTcStages && kTcStagesPerBlock % kTcGenGroup == 0 && kTcDrain % kTcGenGroup == 0,
+static_assert(kTcGenGroup <= kTcStages && (kTcRingGen & (kTcRingGen - 1)) == 0 &&
+                  kTcStagesPerBlock % kTcGenGroup == 0 && kTcDrain % kTcGenGroup == 0,
               "generic stage groups must fit the ring, the node blocks and the accumulation groups");
 static_assert(kTcFacGroup <= kTcStages && kTcStagesPerBlock % kTcFacGroup == 0 && kTcDrain % kTcFacGroup == 0 &&
                   (kTcEBufs & (kTcEBufs - 1)) == 0 && kTcFacGroup <= 2,
@@ -162,7 +169,7 @@ struct TcSmem {
 };
 
 // Node data is double-buffered: block b is read while block b + 1 is written.
-__host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
+__host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt, int ring = kTcStages) {
   // VG here is the weight rows per node buffer (TcDev::wrows)
   TcSmem L;
   L.a_hi = 0;
@@ -171,7 +178,7 @@ __host__ __device__ inline TcSmem tc_smem_layout(int NT, int VG, int Qt) {
   L.b_lo = 2 * kAStageBytes + NT * 2 * kTcNodes * 2;
   L.stage_bytes = 2 * kAStageBytes + 2 * NT * 2 * kTcNodes * 2;
   L.stages = kTcFront;
-  uint32_t off = kTcFront + kTcStages * L.stage_bytes;
+  uint32_t off = kTcFront + (uint32_t)ring * L.stage_bytes;
   L.pos = off;  // [2][3][128] double: x, y, z of the moved nodes
   off += 2 * 3 * kTcBlockNodes * 8;
   L.w = off;  // [2][VG][kWStride] float2
@@ -646,9 +653,8 @@ __device__ inline void tc_final(const TcDev &p, const TcWork &W, const TcUnit &U
 // commits track).
 template <bool kFence>
 __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, uint32_t idesc, int NT,
-                                uint64_t *empty, uint64_t *accfull, uint32_t g, uint32_t st, uint32_t n_stages,
+                                uint64_t *empty, uint64_t *accfull, uint32_t s, uint32_t st, uint32_t n_stages,
                                 uint32_t lane) {
-  const uint32_t s = g % kTcStages;
   if (kFence) ptx::tc_fence_after();
   const uint32_t stage = sbase + L.stages + s * L.stage_bytes;
   // the drain group's first stage overwrites the accumulator; everything is
@@ -694,7 +700,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   uint64_t *empty = reinterpret_cast<uint64_t *>(smem + kTcBars);
-  uint64_t *accfull = empty + kTcStages;
+  uint64_t *gempty = empty + kTcStages;  // the generic ring's slots
+  uint64_t *accfull = gempty + kTcRingGen;
   uint64_t *done = accfull + 1;
   uint64_t *rawfull = done + 1;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kTcMisc);
@@ -707,7 +714,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   const uint32_t sbase = ptx::smem_addr(smem);
 
   if (tid == 0) {
-    for (int s = 0; s < kTcStages; ++s) ptx::mbar_init(&empty[s], 1);
+    for (int s = 0; s < kTcStages + kTcRingGen; ++s) ptx::mbar_init(&empty[s], 1);
     ptx::mbar_init(accfull, 1);
     ptx::mbar_init(done, 1);
     ptx::mbar_init(rawfull, 1);
@@ -738,6 +745,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
   // phase-table thread: q = (tid - 256) / 8 (+ 32), nodes 2 ((tid - 256) % 8) + {0, 1}
   const int tq = (tid - 256) >> 3, tn = ((tid - 256) & 7) * 2;
   uint32_t gst = 0, raw_seq = 0;
+  uint32_t gsg = 0;  // stages of generic units so far (their ring's counter)
   int gbase = 0;
   TcRaw raw;
   for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
@@ -750,7 +758,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     const TcDev &p = B.entries[e_lo];
     const TcWork W = tc_work(p);
     const int NT = p.NT, NH = NT >> 1, VG = p.VG, Qt = p.Qt, WR = p.wrows;
-    const TcSmem L = tc_smem_layout(NT, WR, Qt);
+    const TcSmem L = tc_smem_layout(NT, WR, Qt, p.kind == 0 ? kTcStages : kTcRingGen);
     double *pos_all = reinterpret_cast<double *>(smem + L.pos);
     float2 *w_all = reinterpret_cast<float2 *>(smem + L.w);
     float2 *etab = reinterpret_cast<float2 *>(smem + L.etab);
@@ -827,7 +835,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
     }
     // the first group's tables are read by other warps than their writers
     if (fac) ptx::named_barrier(1, kTcProducers);
-    const uint32_t g0 = gst;
+    const uint32_t g0 = gst, gg0 = gsg;
     int next_drain = 0;
     if (!fac) {
       // ------------------------------------------- generic unit, all warps --
@@ -859,14 +867,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
       for (uint32_t sg = 0; sg < nst; sg += kTcGenGroup) {
         const uint32_t s_end = min(nst, sg + (uint32_t)kTcGenGroup);
         for (uint32_t st = sg; st < s_end; ++st) {
-          const uint32_t g = g0 + st, s = g & (kTcStages - 1);
+          const uint32_t g = gg0 + st, s = g & (kTcRingGen - 1);
           const uint32_t j = st & (kTcStagesPerBlock - 1), blk = st / kTcStagesPerBlock, buf = blk & 1;
           if (loader && blk + 1 < n_blocks && (j == 0 || j == 4))
             tc_stage_block<kModes>(p, U, tid, blk, j == 0, raw, raw_seq, smem + L.raw, rawfull, wrun,
                            pos_all + (buf ^ 1) * 3 * kTcBlockNodes, w_all + (buf ^ 1) * WR * kWStride, abort_flag,
                            rmax);
           // the MMAs that last read stage s were sent at an earlier barrier
-          tc_wait(&empty[s], ((g / kTcStages) & 1) ^ 1, abort_flag);
+          tc_wait(&gempty[s], ((g / kTcRingGen) & 1) ^ 1, abort_flag);
           const uint32_t stg = sstages + s * L.stage_bytes;
           if (g_active) {
             const double *px = pos_all + buf * 3 * kTcBlockNodes + j * kTcNodes + 4 * gc;
@@ -902,7 +910,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         if (warp == 7) {
           ptx::tc_fence_after();
           for (uint32_t st = sg; st < s_end; ++st)
-            tc_issue<false>(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst, lane);
+            tc_issue<false>(L, sbase, tmem, idesc, NT, gempty, accfull, (gg0 + st) & (kTcRingGen - 1), st, nst, lane);
         }
         // an accumulation group ended with this group: fold it before the
         // next group's MMAs (which go out at the next barrier)
@@ -981,7 +989,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         ptx::named_barrier(1, kTcProducers);
         if (warp == 7)
           for (uint32_t st = sg; st < s_end; ++st)
-            tc_issue<true>(L, sbase, tmem, idesc, NT, empty, accfull, g0 + st, st, nst, lane);
+            tc_issue<true>(L, sbase, tmem, idesc, NT, empty, accfull, (g0 + st) % kTcStages, st, nst, lane);
         // an accumulation group ended with this group: fold it before the
         // next group's MMAs go out
         if (s_end < nst && (s_end & (kTcDrain - 1)) == 0) {
@@ -1066,7 +1074,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) signal_tc_kernel(const __grid_c
         }
       }
     }
-    gst = g0 + nst;
+    if (fac) gst = g0 + nst;
+    else gsg = gg0 + nst;
     if (nst > 0) {
       ptx::named_barrier(1, kTcProducers);  // the unit's last stage is written
       if (tid == 0) {
@@ -1572,13 +1581,14 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
       // staging area fits next to the tiles
       const bool aligned = ((uintptr_t)p.r0 % 16 == 0) && ((uintptr_t)p.T2 % 16 == 0) &&
                            ((uintptr_t)p.phi % 16 == 0) && ((uintptr_t)p.MM % 16 == 0);
-      p.tma = aligned && tc_smem_layout(p.NT, p.wrows, p.Qt).total + tc_raw_bytes(p.mm_ld) <= kTcSmemMax;
+      const int ring = kind == 0 ? kTcStages : kTcRingGen;
+      p.tma = aligned && tc_smem_layout(p.NT, p.wrows, p.Qt, ring).total + tc_raw_bytes(p.mm_ld) <= kTcSmemMax;
       // the mode rows of a single POD term of several modes are staged with
       // the node blocks (a rank-1 term is held in registers instead) when
       // they are 16-byte aligned and there is room after the raw block
       if (p.tma && md.kind == FM_MOTION_TERMS && md.n_terms == 1 && md.terms[0].kind != FM_TERM_RESPIRATORY &&
           md.terms[0].n_modes > kTcRegModes && (uintptr_t)md.terms[0].modes % 16 == 0 &&
-          tc_smem_layout(p.NT, p.wrows, p.Qt).total + tc_raw_bytes(p.mm_ld) +
+          tc_smem_layout(p.NT, p.wrows, p.Qt, ring).total + tc_raw_bytes(p.mm_ld) +
                   tc_mode_bytes(3 * md.terms[0].n_modes) <= kTcSmemMax)
         p.mstage = 3 * md.terms[0].n_modes;
     }
@@ -1624,13 +1634,16 @@ static int tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc
   int acc_cols = 32;
   size_t smem = 0;
   bool modes = false;
+  auto staging = [&](const TcDev &d) -> size_t {
+    return d.tma ? tc_raw_bytes(d.mm_ld) + tc_mode_bytes(d.mstage) : 0;
+  };
   for (int e = 0; e < ne; ++e) {
     modes = modes || host[e].mstage != 0;
     int NT = host[e].NT, ac = 32;
     while (ac < NT) ac <<= 1;
     if (ac > acc_cols) acc_cols = ac;
-    const size_t sm = tc_smem_layout(NT, host[e].wrows, host[e].Qt).total +
-                      (host[e].tma ? tc_raw_bytes(host[e].mm_ld) + tc_mode_bytes(host[e].mstage) : 0);
+    const int ring = host[e].kind == 0 ? kTcStages : kTcRingGen;
+    const size_t sm = tc_smem_layout(NT, host[e].wrows, host[e].Qt, ring).total + staging(host[e]);
     if (sm > smem) smem = sm;
   }
   FM_REQUIRE(smem <= kTcSmemMax, FM_ERR_UNSUPPORTED, "%s: tile needs %zu bytes of shared memory", who, smem);
