@@ -117,10 +117,13 @@ class Simulation:
     """Device-resident state of one request.  Construction queues the upload
     and the mass assembly on `stream` and records `ready` there.  `uploaded`:
     the request's inputs already on the device (in _upload_items order), when
-    several requests were sent up together."""
+    several requests were sent up together.  `pinned_kspace`: the k-space
+    frames are allocated in pinned memory and copied there straight from the
+    device (one-shot batches; a serving loop reuses pinned staging instead,
+    which costs no new pinned allocation per request)."""
 
     def __init__(self, req: Request, device: torch.device, stream: torch.cuda.Stream | None = None,
-                 uploaded: list | None = None):
+                 uploaded: list | None = None, pinned_kspace: bool = False):
         from .Assemble import mass_lumped
         from .FiniteElements import FiniteElement, QuadratureRule
         self.req = req
@@ -152,9 +155,10 @@ class Simulation:
             self.ready = torch.cuda.Event()
             self.ready.record(self.stream)
         # k-space frames land in pinned memory straight from the device when
-        # they are small enough (no second host copy), else via staging
+        # asked (one-shot batches: no second host copy) and small enough,
+        # else via pinned staging reused frame after frame
         shape = (req.frames, *t.shape, req.n_coils)
-        if int(np.prod(shape)) * 8 <= PINNED_KSPACE_MAX:
+        if pinned_kspace and int(np.prod(shape)) * 8 <= PINNED_KSPACE_MAX:
             self._kspace_t = torch.empty(shape, dtype=torch.complex64, pin_memory=True)
             self.kspace = self._kspace_t.numpy()
         else:
@@ -313,7 +317,7 @@ def simulate_batch(requests: list[Request], device: torch.device | None = None,
     dev = ops.upload_many(items, device) if items else []
     sims, k = [], 0
     for r, c in zip(requests, counts):
-        sims.append(Simulation(r, device, stream, uploaded=dev[k:k + c]))
+        sims.append(Simulation(r, device, stream, uploaded=dev[k:k + c], pinned_kspace=True))
         k += c
     run_iteration(sims, tuning or SERVING_TUNING)
     return [s.kspace[0] for s in sims]
