@@ -656,7 +656,12 @@ __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, 
                                 uint64_t *empty, uint64_t *accfull, uint32_t s, uint32_t st, uint32_t n_stages,
                                 uint32_t lane) {
   if (kFence) ptx::tc_fence_after();
-  const uint32_t stage = sbase + L.stages + s * L.stage_bytes;
+  // Descriptors (ptx::smem_desc_sw64): the tiles of a stage differ only in
+  // the start-address field, address / 16 (below 2^14 in shared memory, and
+  // every tile and stage offset a multiple of 16), so the stage's field is
+  // formed once and each tile's is one add; the high word is constant.
+  const uint32_t f0 = ((sbase + L.stages + s * L.stage_bytes) >> 4) | (1u << 16);  // + LBO
+  constexpr uint32_t kDescHi = (512u >> 4) | (1u << 14) | (4u << 29);            // SBO, version, 64B swizzle
   // the drain group's first stage overwrites the accumulator; everything is
   // computed before the first MMA goes out
   const uint32_t acc0 = (st % kTcDrain) == 0 ? 0u : 1u;
@@ -664,10 +669,10 @@ __device__ inline void tc_issue(const TcSmem &L, uint32_t sbase, uint32_t tmem, 
 #pragma unroll
   for (int ks = 0; ks < 2; ++ks) {
     // K step ks: elements 16 ks .. 16 ks + 15, bytes 32 ks .. of every row
-    ad[ks][0] = ptx::smem_desc_sw64(stage + L.a_hi + ks * 32);
-    ad[ks][1] = ptx::smem_desc_sw64(stage + L.a_lo + ks * 32);
-    bd[ks][0] = ptx::smem_desc_sw64(stage + L.b_hi + ks * 32);
-    bd[ks][1] = ptx::smem_desc_sw64(stage + L.b_lo + ks * 32);
+    ad[ks][0] = ((uint64_t)kDescHi << 32) | (f0 + ((L.a_hi + ks * 32) >> 4));
+    ad[ks][1] = ((uint64_t)kDescHi << 32) | (f0 + ((L.a_lo + ks * 32) >> 4));
+    bd[ks][0] = ((uint64_t)kDescHi << 32) | (f0 + ((L.b_hi + ks * 32) >> 4));
+    bd[ks][1] = ((uint64_t)kDescHi << 32) | (f0 + ((L.b_lo + ks * 32) >> 4));
   }
   if (tc_narrow(NT)) {
     // A_hi [B_hi; B_lo] (N = 2 NT, both tiles from b_hi on), then A_lo B_hi
