@@ -298,29 +298,53 @@ def run_iteration(sims: list[Simulation], tuning: ops.Tuning = SERVING_TUNING) -
         finish_iteration(launch_iteration(sims, tuning))
 
 
+def _split_by_work(requests: list[Request], parts: int) -> list[list[Request]]:
+    """Consecutive groups of requests with about equal node*k-sample work."""
+    total = sum(r.work for r in requests)
+    groups, cur, acc = [], [], 0.0
+    for r in requests:
+        cur.append(r)
+        acc += r.work
+        if len(groups) < parts - 1 and acc >= total * (len(groups) + 1) / parts:
+            groups.append(cur)
+            cur = []
+    if cur:
+        groups.append(cur)
+    return groups
+
+
 def simulate_batch(requests: list[Request], device: torch.device | None = None,
-                   tuning: ops.Tuning | None = None) -> list[np.ndarray]:
-    """One frame of many simulations, host arrays in and host arrays out: all
-    inputs go up through pinned staging, every Bloch block and coil expansion
-    runs, one persistent tensor-core launch contracts every Signal, and the
-    k-spaces come back through pinned memory.  Returns one (n_ro, n_lines,
-    n_kz, C) complex64 array per request."""
+                   tuning: ops.Tuning | None = None, parts: int = 2) -> list[np.ndarray]:
+    """One frame of many simulations, host arrays in and host arrays out.
+
+    The requests go in `parts` consecutive groups of about equal work.  Each
+    group's inputs go up through pinned staging in one pass (copies on
+    several threads) and one host-to-device transfer.  Its Bloch blocks and
+    coil expansions run, then one persistent tensor-core launch contracts all
+    of its Signals, and the k-spaces come back through pinned memory.  The
+    host stages the next group while the device works on the last one.  A
+    request's result does not depend on its group.  Returns one (n_ro,
+    n_lines, n_kz, C) complex64 array per request."""
     device = device or ops.require_cuda()
     stream = torch.cuda.current_stream(device)
-    # every request's inputs in one staging pass (copies on several threads)
-    # and one host-to-device transfer
-    items, counts = [], []
-    for r in requests:
-        it = _upload_items(r)
-        items += it
-        counts.append(len(it))
-    dev = ops.upload_many(items, device) if items else []
-    sims, k = [], 0
-    for r, c in zip(requests, counts):
-        sims.append(Simulation(r, device, stream, uploaded=dev[k:k + c], pinned_kspace=True))
-        k += c
-    run_iteration(sims, tuning or SERVING_TUNING)
-    return [s.kspace[0] for s in sims]
+    launched = []
+    for group in _split_by_work(requests, max(1, parts)):
+        items, counts = [], []
+        for r in group:
+            it = _upload_items(r)
+            items += it
+            counts.append(len(it))
+        dev = ops.upload_many(items, device) if items else []
+        sims, k = [], 0
+        for r, c in zip(group, counts):
+            sims.append(Simulation(r, device, stream, uploaded=dev[k:k + c], pinned_kspace=True))
+            k += c
+        launched.append((sims, launch_iteration(sims, tuning or SERVING_TUNING)))
+    out = []
+    for sims, it in launched:
+        finish_iteration(it)
+        out += [s.kspace[0] for s in sims]
+    return out
 
 
 def latency_stats(latencies: list[float]) -> dict:
