@@ -298,6 +298,18 @@ def run_iteration(sims: list[Simulation], tuning: ops.Tuning = SERVING_TUNING) -
         finish_iteration(launch_iteration(sims, tuning))
 
 
+_copy_streams: dict = {}
+
+
+def _copy_stream(device: torch.device) -> torch.cuda.Stream:
+    key = device.index if device.index is not None else torch.cuda.current_device()
+    st = _copy_streams.get(key)
+    if st is None:
+        st = torch.cuda.Stream(device=device)
+        _copy_streams[key] = st
+    return st
+
+
 def _split_by_work(requests: list[Request], parts: int) -> list[list[Request]]:
     """Consecutive groups of requests with about equal node*k-sample work."""
     total = sum(r.work for r in requests)
@@ -314,7 +326,7 @@ def _split_by_work(requests: list[Request], parts: int) -> list[list[Request]]:
 
 
 def simulate_batch(requests: list[Request], device: torch.device | None = None,
-                   tuning: ops.Tuning | None = None, parts: int = 2) -> list[np.ndarray]:
+                   tuning: ops.Tuning | None = None, parts: int = 4) -> list[np.ndarray]:
     """One frame of many simulations, host arrays in and host arrays out.
 
     The requests go in `parts` consecutive groups of about equal work.  Each
@@ -322,11 +334,15 @@ def simulate_batch(requests: list[Request], device: torch.device | None = None,
     several threads) and one host-to-device transfer.  Its Bloch blocks and
     coil expansions run, then one persistent tensor-core launch contracts all
     of its Signals, and the k-spaces come back through pinned memory.  The
-    host stages the next group while the device works on the last one.  A
-    request's result does not depend on its group.  Returns one (n_ro,
+    host stages the next group while the device works on the last one, and
+    its transfer (on a copy stream) overlaps that work.  A request's result
+    does not depend on its group.  Returns one (n_ro,
     n_lines, n_kz, C) complex64 array per request."""
     device = device or ops.require_cuda()
     stream = torch.cuda.current_stream(device)
+    # uploads go through a copy stream: a group's transfer overlaps the
+    # previous group's launch, and the launch stream waits for it
+    copy = _copy_stream(device)
     launched = []
     for group in _split_by_work(requests, max(1, parts)):
         items, counts = [], []
@@ -334,7 +350,14 @@ def simulate_batch(requests: list[Request], device: torch.device | None = None,
             it = _upload_items(r)
             items += it
             counts.append(len(it))
-        dev = ops.upload_many(items, device) if items else []
+        dev = []
+        if items:
+            with torch.cuda.stream(copy):
+                dev = ops.upload_many(items, device)
+            ready = torch.cuda.Event()
+            ready.record(copy)
+            stream.wait_event(ready)
+            dev[0].record_stream(stream)  # the views share one allocation
         sims, k = [], 0
         for r, c in zip(group, counts):
             sims.append(Simulation(r, device, stream, uploaded=dev[k:k + c], pinned_kspace=True))
