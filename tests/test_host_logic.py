@@ -298,3 +298,21 @@ def test_gather_data_reduces_host_data_on_cuda_under_nccl():
     assert reduce_device("gloo", host) == torch.device("cpu")
     dev_t = torch.empty(0, device="meta")
     assert reduce_device("nccl", dev_t, current_cuda=0) == torch.device("cuda", 0)
+
+
+def test_simulate_batch_groups_are_consecutive_and_balanced():
+    # simulate_batch stages and launches its requests in groups: every request
+    # in exactly one group, in order, and the groups' work close to equal
+    from types import SimpleNamespace
+    from feelmri_b200.serving import _split_by_work
+    rng = np.random.default_rng(3)
+    reqs = [SimpleNamespace(work=float(w)) for w in rng.uniform(1.0, 10.0, 64)]
+    total = sum(r.work for r in reqs)
+    for parts in (1, 2, 4, 7):
+        groups = _split_by_work(reqs, parts)
+        assert 1 <= len(groups) <= parts
+        assert [r for g in groups for r in g] == reqs
+        if parts > 1:
+            sums = [sum(r.work for r in g) for g in groups]
+            assert max(sums) <= total / parts + 10.0
+    assert _split_by_work([], 3) == []
