@@ -1606,7 +1606,7 @@ static int tc_prepare(const fm_signal_args *a, TcPlan &pl, const fm_tc_tuning *t
 
 // Signal for n problems: per-problem preparation, then one persistent
 // tensor-core launch over all of their work units, then the split sums.
-constexpr int kTcSideStreams = 4;  // helper streams for the per-problem preparations of a batch
+constexpr int kTcSideStreams = 8;  // helper streams for the per-problem preparations of a batch
 
 static int tc_batch(fm_ctx *ctx, const fm_signal_args *probs, int n, const fm_tc_tuning *tune, void *ws,
                     size_t ws_bytes, const char *who) {

@@ -196,12 +196,14 @@ class Simulation:
         return lower(self.req.pod, self.req.n_nodes, self.device)
 
 
-BLOCH_STREAMS = 4  # helper streams over which a set of simulations' Bloch blocks is spread
+BLOCH_STREAMS = 8  # helper streams over which a set of simulations' Bloch blocks is spread
 _side_streams: dict = {}
 
 
-def helper_streams(device: torch.device, k: int = BLOCH_STREAMS) -> list:
-    """k helper streams of `device`, created once and reused."""
+def helper_streams(device: torch.device, k: int | None = None) -> list:
+    """k helper streams of `device` (BLOCH_STREAMS when k is None), created
+    once and reused."""
+    k = BLOCH_STREAMS if k is None else k
     key = (device.index if device.index is not None else torch.cuda.current_device(), k)
     ss = _side_streams.get(key)
     if ss is None:
@@ -224,7 +226,7 @@ def enqueue_bloch_all(sims: list, frames: list | None = None) -> None:
         for i, s in enumerate(sims):
             s.enqueue_bloch(frames[i] if frames is not None else s.frame)
         return
-    side = helper_streams(sims[0].device)[:k]
+    side = helper_streams(sims[0].device, BLOCH_STREAMS)[:k]
     fork = torch.cuda.Event()
     fork.record(main)
     for st in side:
